@@ -1,0 +1,492 @@
+"""Benchmark of forcepho's likelihood hot path (EvaluateProposal) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload batched|limits|multiband|small] [--patches 512]
+
+Workload (default ``batched``): 512 seeded synthetic patches with uneven
+sources (1-30), bands (1-8), exposures per band (1-4) and pixels per exposure
+(32^2-256^2), 4-Gaussian PSFs x 9 Sersic radii; data = model + noise.  A
+*step* evaluates chi2 and its gradient for one proposal on every patch.
+
+Our arm prints one JSON line: ``value`` = pixel-Gaussian evaluations/s of the
+batched persistent kernels (CUDA graph replay, inputs resident in HBM, timed
+with CUDA events); ``e2e`` = the same through ``BatchedProposer.evaluate_proposals``
+with host proposals in and chi2/gradients out every step; ``plain`` = the
+one-launch-per-patch port-equivalent kernel on the same patches;
+``roofline`` = the tile kernel's FP32 work against the FP32 peak measured in
+this run; ``cpu_baseline`` = the reference CPU kernel on a bounded sample.
+
+``--impl reference`` times the reference's own CPU kernel
+(forcepho/src/compute_gaussians_kernel.cc built from source in oracle/_ref)
+on the host cores, on the same workload, and prints its line.
+Multi-GPU (torchrun): each rank evaluates its own batch (weak scaling); the
+only collectives are a barrier and the max of the timings.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("lnlike+grad evals/s and pixel-Gaussian evals/s (batched vs plain, 1 B200, chi2 relerr<=1e-6)")
+UNIT = "pixel-Gaussian evals/s"
+FLOPS_PER_PAIR = 84      # FP32 flops (FMA = 2) of one forward + adjoint pair evaluation
+EX2_PER_PAIR = 2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "limits", "multiband", "small"])
+    ap.add_argument("--patches", type=int, default=512)
+    ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--tile-pixels", type=int, default=0)
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+# ----------------------------------------------------------------------------
+# workload
+# ----------------------------------------------------------------------------
+def workload_shapes(args, rank):
+    """Patch shape draws of the workload (cheap, no pixels)."""
+    from forcepho_b200 import synthetic as S
+    if args.workload == "batched":
+        return [("batched", sh) for sh in S.batched_shapes(seed=4 + 1000 * rank, n_patches=args.patches)]
+    return [(args.workload, {"seed": 1 + 1000 * rank})]
+
+
+def make_patches(args, rank, render_on_gpu=True):
+    """The workload's patches; data rendered by the GPU kernel (model + noise)."""
+    from forcepho_b200 import synthetic as S
+    patches = []
+    for kind, sh in workload_shapes(args, rank):
+        if kind == "batched":
+            rng = np.random.default_rng(sh["seed"])
+            p = S.make_patch(rng, n_sources=sh["n_sources"], exp_per_band=sh["exp_per_band"],
+                             exp_pix=sh["exp_pix"], n_psf=4, source_params=S._broad_source, raster_width=256)
+            p._rng = rng
+        else:
+            p = S.CONFIGS[kind](seed=sh["seed"])
+            p._rng = np.random.default_rng(sh["seed"] + 17)
+        patches.append(p)
+    sigmas = [p._rng.uniform(0.5, 2.0, p.n_exp) for p in patches]
+    models = None
+    if render_on_gpu:
+        from forcepho_b200.batch import render_models
+        models = render_models(patches)
+    for i, p in enumerate(patches):
+        S.add_noise(p, p._rng, sigmas[i], None if models is None else models[i])
+    return patches
+
+
+def perturbed_proposals(patches, seed=99):
+    """Proposals off the truth (non-trivial gradients), fixed per run."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for p in patches:
+        q = p.scene.get_proposal().copy()
+        n = len(q)
+        q["ra"] += rng.normal(0, 2e-6, n).astype(np.float32)
+        q["dec"] += rng.normal(0, 2e-6, n).astype(np.float32)
+        q["q"] = np.clip(q["q"] * rng.uniform(0.95, 1.05, n), 0.2, 0.99).astype(np.float32)
+        out.append(q)
+    return out
+
+
+# ----------------------------------------------------------------------------
+# clocks during the timed region
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# CPU: the reference CPU kernel on a bounded sample
+# ----------------------------------------------------------------------------
+def _cpu_worker_init(root):
+    sys.path.insert(0, root)
+
+
+def _cpu_item(task):
+    """Evaluate one (patch, band) with the reference CPU kernel (or the oracle
+    port when the reference was not built); returns (pairs, seconds)."""
+    from forcepho_b200 import synthetic as S
+    from oracle import oracle as O
+    kind, sh, band, use_ref = task
+    if kind == "batched":
+        rng = np.random.default_rng(sh["seed"])
+        p = S.make_patch(rng, n_sources=sh["n_sources"], exp_per_band=sh["exp_per_band"], exp_pix=sh["exp_pix"],
+                         n_psf=4, source_params=S._broad_source, raster_width=256)
+        S.add_noise(p, rng, rng.uniform(0.5, 2.0, p.n_exp))
+    else:
+        p = S.CONFIGS[kind](seed=sh["seed"])
+    prop = perturbed_proposals([p])[0]
+    hs = O.HostStruct(p)
+    pp = np.ascontiguousarray(prop)
+    e0, ne = int(p.band_start[band]), int(p.band_N[band])
+    pairs = int(np.sum(p.exposure_N[e0:e0 + ne].astype(np.int64))) * int(p.n_sources) * int(p.n_psf_per_source[band])
+    t = time.perf_counter()
+    if use_ref:
+        O.ref_module().EvaluateProposal(band, hs.ptr, pp.ctypes.data)
+    else:
+        import ctypes
+        c = ctypes.c_double()
+        g = np.zeros(30 * 7, np.float32)
+        O.lib().fpo_evaluate_band_f32(hs.ptr, pp.ctypes.data, band, ctypes.addressof(c), g.ctypes.data, 1)
+    return pairs, time.perf_counter() - t
+
+
+def cpu_tasks(args, rank, use_ref):
+    tasks = []
+    for kind, sh in workload_shapes(args, rank):
+        nb = len(sh["exp_per_band"]) if kind == "batched" else None
+        if nb is None:
+            from forcepho_b200 import synthetic as S
+            nb = S.CONFIGS[kind](seed=sh["seed"]).n_bands
+        for b in range(nb):
+            tasks.append((kind, sh, b, use_ref))
+    return tasks
+
+
+def cpu_measure(args, rank, seconds, cores=None):
+    """pairs/s of the reference CPU kernel on the first (patch, band) items of
+    the workload that fit ~`seconds` of wall time on `cores` processes."""
+    import multiprocessing as mp
+    from oracle import oracle as O
+    use_ref = O.ref_available()
+    cores = cores or (os.cpu_count() or 1)
+    tasks = cpu_tasks(args, rank, use_ref)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_cpu_worker_init, initargs=(ROOT,)) as pool:
+        # calibrate on one small item, then size the sample to the time budget
+        pairs0, t0 = pool.apply(_cpu_item, (min(tasks[:64], key=lambda t: np.prod(t[1].get("exp_pix", [1])[:1])),))
+        rate1 = pairs0 / max(t0, 1e-6)
+        budget_pairs = rate1 * cores * seconds
+        sample, acc = [], 0
+        for t in tasks:
+            if acc >= budget_pairs:
+                break
+            sample.append(t)
+            kind, sh, b = t[0], t[1], t[2]
+            if kind == "batched":
+                e0 = sum(sh["exp_per_band"][:b])
+                npx = sum(((n + 31) // 32) * 32 for n in sh["exp_pix"][e0:e0 + sh["exp_per_band"][b]])
+                acc += npx * sh["n_sources"] * 36
+            else:
+                acc = budget_pairs
+        wall = time.perf_counter()
+        res = pool.map(_cpu_item, sample, chunksize=1)
+        wall = time.perf_counter() - wall
+    pairs = sum(r[0] for r in res)
+    return {"value": pairs / wall, "unit": UNIT, "cores": cores, "kind": "reference" if use_ref else "port",
+            "sample": "%d (patch, band) items of the %s workload (first in order), %.3g pairs, %.1f s wall on "
+                      "%d processes; data noise-only (work does not depend on pixel values)"
+                      % (len(sample), args.workload, pairs, wall, cores),
+            "pairs": pairs, "seconds": wall}
+
+
+# ----------------------------------------------------------------------------
+# arms
+# ----------------------------------------------------------------------------
+def config_of(args, n_patches, extra=None):
+    c = {"workload": args.workload, "patches_per_gpu": n_patches,
+         "shape_draws": "sources U{1..30}, bands U{1..8}, exposures/band U{1..4}, pixels/exposure U{32^2..256^2}"
+         if args.workload == "batched" else args.workload,
+         "psf": "4 Gaussians x 9 Sersic radii" if args.workload == "batched" else "per workload",
+         "l2": "inputs larger than L2 (pixel arrays of the batch exceed 126 MB)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if world > 1 and rank != 0:
+        return
+    per_step = max(3.0, min(20.0, 150.0 / max(1, args.steps + args.warmup)))
+    samples = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_measure(args, 0, per_step)
+        if i >= args.warmup:
+            samples.append(r)
+    pairs = sum(s["pairs"] for s in samples)
+    secs = sum(s["seconds"] for s in samples)
+    val = pairs / secs
+    cb = dict(samples[-1])
+    cb["value"] = val
+    out = {"metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / len(samples),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic", "config": config_of(args, args.patches),
+           "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+           "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    from forcepho_b200 import _native as N
+    from forcepho_b200.batch import BatchedProposer
+    from forcepho_b200.proposal import PlainProposer
+    import ctypes
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t)
+        return float(t.item())
+
+    t_setup = time.perf_counter()
+    patches = make_patches(args, rank)
+    for p in patches:
+        p.return_residual = False
+        p.send_to_device()
+    proposals = perturbed_proposals(patches)
+    tp = args.tile_pixels or 1024
+    bp = BatchedProposer(patches, tile_pixels=tp, autotune=not args.no_autotune and not args.tile_pixels)
+    bp.set_proposals_async(proposals)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t_setup
+    n_pairs = bp.n_pairs
+    stream = torch.cuda.current_stream()
+
+    # peaks of this device (roofline denominators)
+    L = N.load()
+    scratch = torch.zeros(256, dtype=torch.float32, device="cuda")
+    fp32_tflops, ex2_rate = ctypes.c_double(), ctypes.c_double()
+    N.check(L.fp_measure_peaks(ctypes.c_void_p(scratch.data_ptr()), ctypes.byref(fp32_tflops),
+                               ctypes.byref(ex2_rate), ctypes.c_void_p(stream.cuda_stream)), "fp_measure_peaks")
+
+    # census: pairs evaluated after culling, pairs within the cutoff
+    evaluated, active, dropped = bp.count_pairs()
+
+    # ---- device-resident timing: graph replay of the whole evaluation ----
+    for _ in range(args.warmup):
+        bp.run(stream)
+    torch.cuda.synchronize()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    props_dev = torch.cuda.get_device_properties(dev)
+    gpu_id = ("GPU-" + str(props_dev.uuid)) if getattr(props_dev, "uuid", None) else str(dev)
+    with ClockSampler(gpu_id) as clk:
+        torch.cuda.synchronize()
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            bp.run(stream)
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms_max = max_over_ranks(ms)
+    total_pairs = sum_over_ranks(float(n_pairs))
+    total_patches = sum_over_ranks(float(len(patches)))
+    value = total_pairs / (ms_max * 1e-3)
+    clocks = clk.summary()
+
+    # ---- the tile kernel alone (roofline) ----
+    lp_tiles = N.Launch(bp.launch.tile_pixels, bp.launch.ctas_per_sm, bp.launch.flags, N.PHASE_TILES)
+    bp.plan.evaluate(bp.launch, stream=stream)          # setup tables current
+    for _ in range(2):
+        bp.plan.evaluate(lp_tiles, stream=stream)
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0.record(stream)
+    for _ in range(args.steps):
+        bp.plan.evaluate(lp_tiles, stream=stream)
+    k1.record(stream)
+    k1.synchronize()
+    tile_ms = k0.elapsed_time(k1) / args.steps
+    achieved = FLOPS_PER_PAIR * active / (tile_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_tflops.value, "unit": "TFLOP/s",
+                "frac": achieved / fp32_tflops.value, "traffic": None,
+                "kernel": "tile_kernel<%d>" % (bp.tile_pixels // 256),
+                "kernel_ms": tile_ms, "share_of_step": tile_ms / ms,
+                "peak_source": "measured in this run: FFMA-chain kernel (fp_measure_peaks), not in MEASURED_PEAKS.json",
+                "work": "84 FP32 flops per pair within the MAX_EXP_ARG cutoff (%d of %d pairs); the culled kernel "
+                        "evaluates %d pairs" % (active, n_pairs, evaluated),
+                "ex2": {"achieved_per_s": EX2_PER_PAIR * active / (tile_ms * 1e-3), "peak_per_s": ex2_rate.value,
+                        "frac": EX2_PER_PAIR * active / (tile_ms * 1e-3) / ex2_rate.value},
+                "hbm_gbs": 16.0 * sum(int(np.sum(p.exposure_N)) for p in patches) / (tile_ms * 1e-3) / 1e9}
+
+    # ---- end to end through the public API (host proposals in, results out) ----
+    for _ in range(2):
+        bp.evaluate_proposals(proposals)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        res = bp.evaluate_proposals(proposals)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    e2e = {"value": total_pairs / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": bp.h2d_bytes,
+           "d2h_bytes_per_step": bp.d2h_bytes, "ms_per_step": e2e_ms,
+           "lnlike_grad_evals_per_s": total_patches / (e2e_ms * 1e-3),
+           "api": "BatchedProposer.evaluate_proposals (pinned H2D of proposals, graph replay, D2H of chi2 + "
+                  "Response records, host sync)"}
+
+    # ---- the plain one-launch-per-patch comparator on the same patches ----
+    plain = PlainProposer()
+    d_prop = torch.zeros((len(patches), 30 * 264), dtype=torch.uint8, device="cuda")
+    d_prop.copy_(bp.plan.proposals.view(len(patches), -1))
+    d_chi2 = torch.zeros((len(patches), 30), dtype=torch.float64, device="cuda")
+    d_resp = torch.zeros((len(patches), 30, 210), dtype=torch.float32, device="cuda")
+
+    def plain_step():
+        for i, p in enumerate(patches):
+            plain.launch(p, d_prop[i].data_ptr(), d_chi2[i].data_ptr(), d_resp[i].data_ptr(), stream)
+
+    plain_step()
+    torch.cuda.synchronize()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    for _ in range(args.plain_steps):
+        plain_step()
+    q1.record(stream)
+    q1.synchronize()
+    plain_ms = max_over_ranks(q0.elapsed_time(q1) / args.plain_steps)
+    # equal results: batched vs plain on every patch
+    bres = bp.evaluate_proposals(proposals)
+    pc, pr = d_chi2.cpu().numpy(), d_resp.cpu().numpy()
+    worst_c, worst_g = 0.0, 0.0
+    for i, p in enumerate(patches):
+        c_b, g_b = bres[i]
+        c_p = pc[i, :p.n_bands]
+        g_p = pr[i].reshape(30, 30, 7)[:p.n_bands, :int(p.n_sources)]
+        scale = np.sum(np.abs(c_b)) + 1.0
+        worst_c = max(worst_c, float(np.max(np.abs(c_b - c_p)) / scale))
+        den = np.linalg.norm(g_b) + 1e-30
+        worst_g = max(worst_g, float(np.linalg.norm(g_b - g_p) / den))
+    plain_out = {"value": total_pairs / (plain_ms * 1e-3), "unit": UNIT, "ms_per_step": plain_ms,
+                 "launches_per_step": len(patches), "speedup_batched_over_plain": plain_ms / ms_max,
+                 "max_chi2_diff_vs_batched": worst_c, "max_grad_normdiff_vs_batched": worst_g}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_measure(args, rank, args.cpu_seconds)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+               "config": config_of(args, len(patches), {"tile_pixels": bp.tile_pixels,
+                                                        "ctas_per_sm": bp.launch.ctas_per_sm,
+                                                        "pairs_per_step_per_gpu": n_pairs,
+                                                        "parallelism": "replicas-%d (independent patch batches)"
+                                                                       % world}),
+               "lnlike_grad_evals_per_s": total_patches / (ms_max * 1e-3),
+               "e2e": e2e, "plain": plain_out, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+               "gpu_launches": 3 * args.steps,
+               "pairs": {"total": n_pairs, "evaluated_after_cull": evaluated, "within_cutoff": active,
+                         "within_cutoff_but_culled": dropped},
+               "autotune": [list(r[1:]) for r in bp.tune_log], "setup_s": setup_s}
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

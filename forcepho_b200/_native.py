@@ -1,0 +1,124 @@
+"""ctypes binding of the C ABI in ``include/forcepho_b200.h``.
+
+The CUDA library is the only compute path: if it is missing and cannot be
+built, importing the device modules raises instead of falling back to
+anything else.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+from .structs import STRUCT_SIZES
+
+c_i32, c_i64, c_vp, c_sz = ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p, ctypes.c_size_t
+
+
+class PatchShape(ctypes.Structure):
+    _fields_ = [("n_bands", c_i32), ("n_exposures", c_i32), ("n_sources", c_i32), ("n_pix", c_i32),
+                ("exposure_start", c_vp), ("exposure_N", c_vp), ("band_start", c_vp),
+                ("band_N", c_vp), ("n_psf_per_source", c_vp)]
+
+
+class PlanSizes(ctypes.Structure):
+    _fields_ = [("n_exposures", c_i64), ("n_tiles", c_i64), ("n_band_outputs", c_i64),
+                ("n_gauss", c_i64), ("n_pairs", c_i64), ("n_partials", c_i64),
+                ("max_gauss", c_i64), ("workspace_bytes", c_i64)]
+
+
+class Launch(ctypes.Structure):
+    _fields_ = [("tile_pixels", c_i32), ("ctas_per_sm", c_i32), ("flags", c_i32), ("phases", c_i32)]
+
+
+FLAG_NO_CULL = 1
+FLAG_STATIC = 2
+PHASE_SETUP, PHASE_TILES, PHASE_REDUCE = 1, 2, 4
+
+# return codes (include/forcepho_b200.h)
+FP_OK, FP_ERR_ARGUMENT, FP_ERR_LIMITS, FP_ERR_CUDA, FP_ERR_WORKSPACE, FP_ERR_DEVICE = 0, -1, -2, -3, -4, -5
+
+# numpy mirrors of the plan tables (filled on the host, copied to the device)
+exposure_desc_dtype = np.dtype([("gauss_offset", np.int64), ("patch", np.int32), ("exposure", np.int32),
+                                ("band", np.int32), ("n_gauss", np.int32), ("n_psf", np.int32),
+                                ("n_sources", np.int32)])
+tile_dtype = np.dtype([("partial_offset", np.int64), ("expo", np.int32), ("pix_start", np.int32),
+                       ("n_pix", np.int32), ("pad", np.int32), ("bbox", np.float32, 4)])
+band_desc_dtype = np.dtype([("patch", np.int32), ("band", np.int32), ("tile_begin", np.int32),
+                            ("tile_end", np.int32), ("n_sources", np.int32), ("pad", np.int32)])
+assert exposure_desc_dtype.itemsize == 32 and tile_dtype.itemsize == 40 and band_desc_dtype.itemsize == 24
+
+# every entry point of include/forcepho_b200.h with its ctypes signature
+SIGNATURES = {
+    "fp_error_string": (ctypes.c_char_p, []),
+    "fp_version": (ctypes.c_int, []),
+    "fp_struct_sizes": (ctypes.c_int, [c_vp]),
+    "fp_evaluate_proposal_plain": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp]),
+    "fp_plan_count": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PlanSizes)]),
+    "fp_plan_fill": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp, c_vp]),
+    "fp_plan_bbox": (ctypes.c_int, [c_vp, c_vp, c_vp, c_i64, c_vp]),
+    "fp_tile_smem_bytes": (ctypes.c_int, [ctypes.c_int, c_i64, ctypes.POINTER(c_i64)]),
+    "fp_evaluate_batch": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.POINTER(PlanSizes), c_vp, c_vp, c_vp,
+                                         c_vp, c_vp, c_vp, c_vp, c_vp, c_sz, ctypes.POINTER(Launch), c_vp]),
+    "fp_read_status": (ctypes.c_int, [c_vp, ctypes.POINTER(c_i32), c_vp]),
+    "fp_count_pairs": (ctypes.c_int, [c_vp, ctypes.POINTER(PlanSizes), c_vp, c_vp, c_vp, c_sz, c_vp, c_vp]),
+    "fp_measure_peaks": (ctypes.c_int, [c_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                        c_vp]),
+}
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib_path():
+    return _build.LIB
+
+
+def load(build_if_missing=True):
+    """Load (building first if needed) the CUDA library and check its struct sizes."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if build_if_missing:
+        _build.build()
+    if not os.path.exists(_build.LIB):
+        raise NativeError("CUDA library %s is missing; run python -m forcepho_b200.build" % _build.LIB)
+    L = ctypes.CDLL(_build.LIB)
+    for name, (res, args) in SIGNATURES.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    sizes = np.zeros(4, dtype=np.int32)
+    L.fp_struct_sizes(sizes.ctypes.data)
+    want = [STRUCT_SIZES["patch"], STRUCT_SIZES["source"], STRUCT_SIZES["response"], STRUCT_SIZES["psf"]]
+    if list(sizes) != want:
+        raise NativeError("struct sizes of %s are %s, expected %s" % (_build.LIB, list(sizes), want))
+    _lib = L
+    return L
+
+
+def check(rc, what=""):
+    """Raise NativeError with the library's message when rc != 0."""
+    if rc != 0:
+        msg = load().fp_error_string().decode(errors="replace")
+        raise NativeError("%s failed (%d): %s" % (what, rc, msg))
+    return rc
+
+
+def patch_shape(patch):
+    """PatchShape of a PatchBase; keeps the index arrays alive on the returned object."""
+    keep = [np.ascontiguousarray(patch.exposure_start, dtype=np.int32),
+            np.ascontiguousarray(patch.exposure_N, dtype=np.int32),
+            np.ascontiguousarray(patch.band_start, dtype=np.int16),
+            np.ascontiguousarray(patch.band_N, dtype=np.int16),
+            np.ascontiguousarray(patch.n_psf_per_source, dtype=np.int32)]
+    s = PatchShape(patch.n_bands, patch.n_exp, int(patch.n_sources), patch.npix,
+                   keep[0].ctypes.data, keep[1].ctypes.data, keep[2].ctypes.data, keep[3].ctypes.data,
+                   keep[4].ctypes.data)
+    s._keep = keep
+    return s

@@ -1,0 +1,195 @@
+"""Many patches, one pass: the batched evaluation of the likelihood hot path.
+
+The reference evaluates one patch per call: ``GPUProposer.evaluate_proposal``
+launches ``EvaluateProposal`` with one CTA per band (forcepho/proposal.py:96-152)
+and scales out by farming patches to MPI ranks (forcepho/dispatcher.py:156-300).
+On a B200 a single patch of a few bands fills a handful of the 148 SMs, so
+``BatchedProposer`` evaluates one proposal for each of many device-resident
+patches in one pass: a single work plan over all their pixel tiles, one
+persistent tile launch, and a fixed-order reduction per (patch, band).  The
+three launches of one evaluation are captured once into a CUDA graph and
+replayed.
+
+``evaluate_proposals(list of source_struct arrays)`` is the public call:
+host proposals -> pinned staging -> device, graph replay, chi2 and Response
+records back to the host, returned per patch in the reference's shapes.
+"""
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .autotune import Autotuner, size_class
+from .device import Plan, pack_proposals, response_view
+from .kernel_limits import MAXBANDS, MAXSOURCES, NPARAMS
+from .structs import source_struct_dtype
+
+__all__ = ["BatchedProposer", "render_models"]
+
+
+class BatchedProposer:
+    """One proposal per patch for a list of device patches (``send_to_device``-ed).
+
+    Parameters
+    ----------
+    patches : list of patches with ``B200PatchMixin``
+    tile_pixels, ctas_per_sm : launch parameters; ``autotune=True`` times the
+        candidates on the device and keeps the fastest.
+    use_graph : capture the evaluation into a CUDA graph on first use.
+    """
+
+    def __init__(self, patches, tile_pixels=1024, ctas_per_sm=3, flags=0, autotune=False,
+                 use_graph=True, tuner=None):
+        N.load()
+        self.patches = list(patches)
+        self.n = len(self.patches)
+        self.flags = flags
+        self.use_graph = use_graph
+        self.graph = None
+        self.tune_log = []
+        if autotune:
+            tuner = tuner or Autotuner()
+            self._autotune(tuner)
+        else:
+            self.plan = Plan(self.patches, tile_pixels=tile_pixels)
+            self.launch = self.plan.launch(ctas_per_sm=ctas_per_sm, flags=flags)
+        self._pin_prop = torch.zeros(self.plan.proposals.numel(), dtype=torch.uint8).pin_memory()
+        self._pin_chi2 = torch.zeros(self.plan.chi2.shape, dtype=torch.float64).pin_memory()
+        self._pin_resp = torch.zeros(self.plan.response.shape, dtype=torch.float32).pin_memory()
+
+    # --- launch parameters ---
+    def _autotune(self, tuner):
+        props = self._current_proposals()
+
+        def make_plan(tp):
+            pl = Plan(self.patches, tile_pixels=tp)
+            pl.proposals.copy_(torch.from_numpy(props.view(np.uint8).reshape(-1)))
+            return pl
+
+        probe = Plan(self.patches, tile_pixels=1024)
+        key = size_class(probe.n_pairs, probe.sizes.n_tiles)
+        del probe
+        tp, cps, ms = tuner.tune(key, make_plan)
+        self.tune_log = [r for r in tuner.log if r[0] == key]
+        self.plan = Plan(self.patches, tile_pixels=tp)
+        self.launch = self.plan.launch(ctas_per_sm=cps, flags=self.flags)
+        self.plan.proposals.copy_(torch.from_numpy(props.view(np.uint8).reshape(-1)))
+
+    def _current_proposals(self):
+        return pack_proposals([p.scene.get_proposal() if getattr(p, "scene", None) is not None
+                               else np.zeros(int(p.n_sources), source_struct_dtype) for p in self.patches],
+                              self.n)
+
+    @property
+    def n_pairs(self):
+        return self.plan.n_pairs
+
+    @property
+    def tile_pixels(self):
+        return self.plan.tile_pixels
+
+    # --- device-side pieces (no host synchronisation) ---
+    def set_proposals_async(self, proposals, stream=None):
+        """Stage host proposals (list of arrays) and queue their copy to the device."""
+        host = pack_proposals(proposals, self.n)
+        self._pin_prop.numpy()[:] = host.view(np.uint8).reshape(-1)
+        s = stream or torch.cuda.current_stream()
+        with torch.cuda.stream(s):
+            self.plan.proposals.copy_(self._pin_prop, non_blocking=True)
+
+    def run(self, stream=None):
+        """Queue one evaluation of the device proposals (graph replay when captured)."""
+        s = stream or torch.cuda.current_stream()
+        if self.use_graph:
+            if self.graph is None:
+                self.capture(s)
+            with torch.cuda.stream(s):
+                self.graph.replay()
+        else:
+            self.plan.evaluate(self.launch, stream=s)
+
+    def capture(self, stream=None):
+        s = stream or torch.cuda.current_stream()
+        # one eager evaluation first: sets kernel attributes outside capture
+        self.plan.evaluate(self.launch, stream=s)
+        s.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.plan.evaluate(self.launch)
+        torch.cuda.synchronize()
+        self.graph = g
+        return g
+
+    def fetch_async(self, stream=None):
+        s = stream or torch.cuda.current_stream()
+        with torch.cuda.stream(s):
+            self._pin_chi2.copy_(self.plan.chi2, non_blocking=True)
+            self._pin_resp.copy_(self.plan.response, non_blocking=True)
+
+    def results(self):
+        """Per patch (chi2[n_bands] f64, dchi2[n_bands, n_sources, 7] f32) from the last fetch."""
+        c = self._pin_chi2.numpy()
+        r = self._pin_resp.numpy()
+        out = []
+        for i, p in enumerate(self.patches):
+            out.append((c[i, :p.n_bands].copy(), response_view(r[i], p.n_bands, int(p.n_sources)).copy()))
+        return out
+
+    # --- the public call ---
+    def evaluate_proposals(self, proposals, stream=None):
+        """Evaluate one proposal (``source_struct_dtype`` array) per patch.
+
+        Returns a list of (chi2, chi2_derivs) per patch with the shapes
+        ``GPUProposer.evaluate_proposal`` returns."""
+        s = stream or torch.cuda.current_stream()
+        self.set_proposals_async(proposals, s)
+        self.run(s)
+        self.fetch_async(s)
+        s.synchronize()
+        return self.results()
+
+    # --- transfer accounting of one evaluate_proposals call ---
+    @property
+    def h2d_bytes(self):
+        return int(self.plan.proposals.numel())
+
+    @property
+    def d2h_bytes(self):
+        return int(self.plan.chi2.numel() * 8 + self.plan.response.numel() * 4)
+
+    def count_pairs(self, stream=None):
+        """(evaluated pairs, pairs within the cutoff, within-cutoff pairs culled) of one evaluation."""
+        import ctypes
+        s = stream or torch.cuda.current_stream()
+        self.plan.evaluate(self.launch, stream=s)
+        counts = torch.zeros(3, dtype=torch.int64, device=self.plan.device)
+        pl = self.plan
+        N.check(pl.L.fp_count_pairs(pl.d_patches.data_ptr(), ctypes.byref(pl.sizes), pl.d_expos.data_ptr(),
+                                    pl.d_tiles.data_ptr(), pl.workspace.data_ptr(), pl.workspace.numel(),
+                                    counts.data_ptr(), ctypes.c_void_p(s.cuda_stream)), "fp_count_pairs")
+        s.synchronize()
+        return tuple(int(v) for v in counts.cpu())
+
+
+def render_models(patches, proposals=None, tile_pixels=1024):
+    """Model counts of every pixel of every (device) patch at ``proposals``
+    (default: each patch's scene), rendered by the tiled kernel as minus the
+    residual of an all-zero data array.  Returns a list of f32 host arrays."""
+    saved = []
+    for p in patches:
+        saved.append((p.data, p.return_residual))
+        p.data = np.zeros_like(p.data)
+        p.return_residual = True
+        p.send_to_device()
+    bp = BatchedProposer(patches, tile_pixels=tile_pixels, use_graph=False)
+    props = proposals or [p.scene.get_proposal() for p in patches]
+    bp.evaluate_proposals(props)
+    models = [-p.retrieve_array("residual") for p in patches]
+    for p, (d, rr) in zip(patches, saved):
+        p.data = d
+        p.return_residual = rr
+        p.free()
+    return models
+
+
+_ = (MAXBANDS, MAXSOURCES, NPARAMS)

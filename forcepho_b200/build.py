@@ -1,0 +1,72 @@
+"""Compile the CUDA library ``forcepho_b200/lib/libforcepho_b200.so`` in-tree.
+
+    python -m forcepho_b200.build [--verbose]
+
+nvcc builds every ``csrc/*.cu`` for sm_100a only (``-gencode
+arch=compute_100a,code=sm_100a``) into one shared library exporting the C ABI
+of ``include/forcepho_b200.h``.  The library is rebuilt only when a source or
+header is newer than it (or with ``force=True``).
+"""
+
+import glob
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIBDIR = os.path.join(PKG, "lib")
+LIB = os.path.join(LIBDIR, "libforcepho_b200.so")
+INCLUDE = os.path.join(ROOT, "include")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",
+              "-shared", "--expt-relaxed-constexpr", "-I", INCLUDE]
+
+
+def nvcc():
+    for cand in [os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc"]:
+        if cand and os.path.exists(cand):
+            return cand
+    return "nvcc"
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+
+
+def _deps():
+    return sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+
+
+def up_to_date():
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(f) <= t for f in _deps())
+
+
+def build(force=False, verbose=False, extra=()):
+    """Build the library if needed; returns its path."""
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(LIBDIR, exist_ok=True)
+    tmp = LIB + ".tmp"
+    cmd = [nvcc()] + ARCH + NVCC_FLAGS + list(extra) + ["-o", tmp] + sources() + ["-lcudart"]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if verbose or r.returncode:
+        sys.stdout.write(r.stdout)
+        sys.stderr.write(r.stderr)
+    if r.returncode:
+        raise RuntimeError("nvcc failed building %s (exit %d)" % (LIB, r.returncode))
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force=True, verbose="--verbose" in sys.argv)
+    print(LIB)

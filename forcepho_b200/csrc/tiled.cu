@@ -1,0 +1,711 @@
+// tiled.cu -- the B200 path: image-Gaussian setup in FP64, one persistent
+// launch over (patch, exposure, pixel-tile) work items, fixed-order reduction.
+//
+// Per evaluation (all on one stream, no host synchronisation):
+//   setup_kernel   one CTA per exposure: every image Gaussian of the exposure in
+//                  FP64 (fp_gauss.cuh), stored as FP32 pixel-loop parameters with
+//                  the ex2 scale folded in, an FP32 bounding box of its
+//                  E = dx^T F dx <= MAX_EXP_ARG region, and the FP64 Jacobian.
+//   tile_kernel    persistent CTAs pop tiles (largest first).  Per tile:
+//                  1. cull: keep the Gaussians whose box meets the tile's pixel
+//                     box (every other Gaussian has E > MAX_EXP_ARG at every
+//                     pixel of the tile and contributes exactly nothing);
+//                  2. forward, pixel-parallel: P pixels per thread, Gaussians
+//                     streamed from shared memory, SFU ex2, FP32 runs of
+//                     FP_RUN Gaussians flushed into per-pixel FP64 sums;
+//                     residual, chi2 term in f64, w = r ierr^2;
+//                  3. adjoint, Gaussian-parallel: one Gaussian per lane, the
+//                     tile's nonzero-weight pixels broadcast from shared memory;
+//                     each lane accumulates 12 moments (FP32 runs -> FP64) from
+//                     which the 6 image-space partials follow exactly; the FP64
+//                     Jacobian maps them to the 7 on-sky partials once per
+//                     Gaussian, not once per pixel;
+//                  4. per-source sums in a fixed order -> per-tile partials.
+//   reduce_kernel  per (patch, band): partials summed over the band's tiles in
+//                  canonical order (FP64) -> chi2 (f64) and Response (f32).
+// No atomics touch the results, so they are bitwise reproducible.
+
+#include "fp_common.cuh"
+#include "fp_gauss.cuh"
+
+namespace {
+
+constexpr int SLOT_GROUPS = FP_CHUNK / 32 + FP_WARPS - 1;   // adjoint result slots per lane
+
+// ---------------------------------------------------------------------------
+// setup
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+setup_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc *__restrict__ expos,
+             const fp_source *__restrict__ proposals, float4 *__restrict__ gfwd,
+             float4 *__restrict__ gbox, double *__restrict__ gjac, fp_control *ctl)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->queue = 0ULL;   // work queue of tile_kernel
+    const fp_exposure_desc ed = expos[blockIdx.x];
+    const fp_patch *pt = patches[ed.patch];
+    if (ed.n_sources > MAXSOURCES || pt->n_sources != ed.n_sources) {
+        if (threadIdx.x == 0) atomicOr(&ctl->status, FP_STATUS_SOURCES);
+        return;
+    }
+    const fp_source *srcs = proposals + (size_t)ed.patch * MAXSOURCES;
+    const double c = FP_EXP2_SCALE;
+    for (int g = threadIdx.x; g < ed.n_gauss; g += blockDim.x) {
+        fp_img_gauss<double> G;
+        fp_make_gaussian<double>(pt, srcs, ed.band, ed.exposure, g, ed.n_psf, G);
+        const int64_t i = ed.gauss_offset + g;
+        const float xc = (float)G.xcen, yc = (float)G.ycen;
+        const float fxs = (float)(c * G.fxx), fys = (float)(c * G.fyy), fxys = (float)(c * G.fxy);
+        const double k0 = 1.0 - (G.fxx + G.fyy) / 24.0;
+        gfwd[2 * i] = make_float4(xc, yc, fxs, fxys);
+        gfwd[2 * i + 1] = make_float4(fys, (float)(G.amp * k0), (float)(G.amp * FP_C24), (float)k0);
+
+        // box of {E <= MAX_EXP_ARG} for the FP32 parameters the pixel loops use,
+        // widened by 1% in E and 1e-3 px so FP32 rounding of E cannot reach past it
+        const double Fxx = (double)fxs / c, Fyy = (double)fys / c, Fxy = (double)fxys / c;
+        const double det = Fxx * Fyy - Fxy * Fxy;
+        float4 box = make_float4(-INFINITY, INFINITY, -INFINITY, INFINITY);   // never culled
+        if (isfinite(xc) && isfinite(yc) && isfinite(det) && det > 0.0 && Fxx > 0.0 && Fyy > 0.0) {
+            const double lim = MAX_EXP_ARG * 1.01;
+            const double hx = sqrt(lim * Fyy / det) + 1e-3, hy = sqrt(lim * Fxx / det) + 1e-3;
+            box = make_float4(__double2float_rd((double)xc - hx), __double2float_ru((double)xc + hx),
+                              __double2float_rd((double)yc - hy), __double2float_ru((double)yc + hy));
+        }
+        gbox[i] = box;
+
+        double *J = gjac + (size_t)FP_JAC * i;
+        J[0] = G.amp; J[1] = G.fxx; J[2] = G.fxy; J[3] = G.fyy;
+        J[4] = G.dA_dflux; J[5] = G.dx_dra; J[6] = G.dy_dra; J[7] = G.dx_ddec; J[8] = G.dy_ddec;
+        J[9] = G.dA_dq; J[10] = G.dfxx_dq; J[11] = G.dfyy_dq; J[12] = G.dfxy_dq;
+        J[13] = G.dA_dpa; J[14] = G.dfxx_dpa; J[15] = G.dfyy_dpa; J[16] = G.dfxy_dpa;
+        J[17] = G.dA_dsersic; J[18] = G.dA_drh; J[19] = 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// tile bounding boxes (one-time, per plan)
+// ---------------------------------------------------------------------------
+__global__ void bbox_kernel(const fp_patch *const *__restrict__ patches,
+                            const fp_exposure_desc *__restrict__ expos, fp_tile *tiles, int64_t n_tiles)
+{
+    const int64_t t = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    if (t >= n_tiles) return;
+    const int lane = threadIdx.x & 31;
+    const fp_tile tl = tiles[t];
+    const fp_patch *pt = patches[expos[tl.expo].patch];
+    float x0 = INFINITY, x1 = -INFINITY, y0 = INFINITY, y1 = -INFINITY;
+    for (int i = lane; i < tl.n_pix; i += 32) {
+        const float x = pt->xpix[tl.pix_start + i], y = pt->ypix[tl.pix_start + i];
+        x0 = fminf(x0, x); x1 = fmaxf(x1, x);
+        y0 = fminf(y0, y); y1 = fmaxf(y1, y);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        x0 = fminf(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+        x1 = fmaxf(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+        y0 = fminf(y0, __shfl_xor_sync(0xffffffffu, y0, o));
+        y1 = fmaxf(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+    }
+    if (lane == 0) {
+        tiles[t].bbox[0] = x0; tiles[t].bbox[1] = x1;
+        tiles[t].bbox[2] = y0; tiles[t].bbox[3] = y1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// tile kernel helpers
+// ---------------------------------------------------------------------------
+template <int P>
+__device__ __forceinline__ void load_px(const float *__restrict__ src, bool vec, int nval, float (&v)[P])
+{
+    if (vec && nval >= P) {
+        if constexpr (P == 4) {
+            const float4 t = __ldg(reinterpret_cast<const float4 *>(src));
+            v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+        } else if constexpr (P == 2) {
+            const float2 t = __ldg(reinterpret_cast<const float2 *>(src));
+            v[0] = t.x; v[1] = t.y;
+        } else {
+            v[0] = __ldg(src);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < P; ++k) v[k] = (k < nval) ? __ldg(src + k) : 0.f;
+    }
+}
+
+template <int P>
+__device__ __forceinline__ void store_px(float *dst, bool vec, int nval, const float (&v)[P])
+{
+    if (vec && nval >= P) {
+        if constexpr (P == 4) {
+            *reinterpret_cast<float4 *>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+        } else if constexpr (P == 2) {
+            *reinterpret_cast<float2 *>(dst) = make_float2(v[0], v[1]);
+        } else {
+            dst[0] = v[0];
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < P; ++k)
+            if (k < nval) dst[k] = v[k];
+    }
+}
+
+// Adjoint moments of one Gaussian (params A, B) over pixels [p0, p1) of the
+// tile's nonzero-weight list.  With K = w' 2^(cE) (w' = -2 r ierr^2, zero past
+// the cutoff), H the pixel-integral factor and v' = c F dx:
+//   m0 K, m1 KH, m2 KH vx', m3 KH vy', m4 K vx', m5 K vy', m6 KH dx^2,
+//   m7 KH dy^2, m8 KH dx dy, m9 K dx vx', m10 K dy vy', m11 K (dx vy' + dy vx')
+__device__ __forceinline__ void adjoint_moments(const float4 A, const float4 B,
+                                                const float4 *__restrict__ s_pix, int p0, int p1,
+                                                double (&m)[12])
+{
+    const float xc = A.x, yc = A.y, fxs = A.z, fxys = A.w, fys = B.x, k0 = B.w;
+    const float c24 = (float)FP_C24;
+    for (int r0 = p0; r0 < p1; r0 += FP_RUN) {
+        const int r1 = min(p1, r0 + FP_RUN);
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, a4 = 0.f, a5 = 0.f;
+        float a6 = 0.f, a7 = 0.f, a8 = 0.f, a9 = 0.f, a10 = 0.f, a11 = 0.f;
+#pragma unroll 4
+        for (int p = r0; p < r1; ++p) {
+            const float4 q = s_pix[p];
+            const float dx = q.x - xc, dy = q.y - yc;
+            const float vx = fmaf(fxs, dx, fxys * dy);
+            const float vy = fmaf(fys, dy, fxys * dx);
+            const float pp = dx * vx;
+            const float e = fmaf(dy, vy, pp);
+            const float g = fp_ex2(e);
+            const float K = (e < FP_CUT_SCALED) ? 0.f : q.z * g;
+            const float s = fmaf(vx, vx, vy * vy);
+            const float KH = K * fmaf(s, c24, k0);
+            a0 += K;
+            a1 += KH;
+            a2 = fmaf(KH, vx, a2);
+            a3 = fmaf(KH, vy, a3);
+            a4 = fmaf(K, vx, a4);
+            a5 = fmaf(K, vy, a5);
+            const float hx = KH * dx;
+            a6 = fmaf(hx, dx, a6);
+            a8 = fmaf(hx, dy, a8);
+            a7 = fmaf(KH * dy, dy, a7);
+            a9 = fmaf(K, pp, a9);
+            a10 = fmaf(K, e - pp, a10);
+            a11 = fmaf(K, fmaf(dx, vy, dy * vx), a11);
+        }
+        m[0] += a0; m[1] += a1; m[2] += a2; m[3] += a3; m[4] += a4; m[5] += a5;
+        m[6] += a6; m[7] += a7; m[8] += a8; m[9] += a9; m[10] += a10; m[11] += a11;
+    }
+}
+
+// Image-space partials from the moments (the reference's dC/d{A,x,y,Fxx,Fyy,Fxy}
+// summed over pixels, common_kernel.cc:118-132), then the Jacobian to the 7
+// on-sky partials (common_kernel.cc:135-141), all in FP64.
+__device__ __forceinline__ void moments_to_grad(const double *__restrict__ J, const double (&m)[12],
+                                                double (&g)[NPARAMS])
+{
+    const double amp = J[0], fxx = J[1], fxy = J[2], fyy = J[3];
+    const double ic = 1.0 / FP_EXP2_SCALE;
+    const double SA = m[1];
+    const double Sx = amp * ic * (m[2] - (fxx * m[4] + fxy * m[5]) * (1.0 / 12.0));
+    const double Sy = amp * ic * (m[3] - (fyy * m[5] + fxy * m[4]) * (1.0 / 12.0));
+    const double Sfx = amp * (-0.5 * m[6] - m[0] * (1.0 / 24.0) + ic * m[9] * (1.0 / 12.0));
+    const double Sfy = amp * (-0.5 * m[7] - m[0] * (1.0 / 24.0) + ic * m[10] * (1.0 / 12.0));
+    const double Sfxy = amp * (-m[8] + ic * m[11] * (1.0 / 12.0));
+    g[0] = J[4] * SA;
+    g[1] = J[5] * Sx + J[6] * Sy;
+    g[2] = J[7] * Sx + J[8] * Sy;
+    g[3] = J[9] * SA + J[10] * Sfx + J[12] * Sfxy + J[11] * Sfy;
+    g[4] = J[13] * SA + J[14] * Sfx + J[16] * Sfxy + J[15] * Sfy;
+    g[5] = J[17] * SA;
+    g[6] = J[18] * SA;
+}
+
+struct tile_smem {
+    size_t ga, gb, pix, slot, src, red, ints, idx, total;
+};
+
+__host__ __device__ inline tile_smem tile_smem_layout(int tile_pixels, int max_gauss)
+{
+    tile_smem L;
+    size_t o = 0;
+    L.ga = o;   o += (size_t)FP_CHUNK * 16;
+    L.gb = o;   o += (size_t)FP_CHUNK * 16;
+    L.pix = o;  o += (size_t)tile_pixels * 16;
+    L.slot = o; o += (size_t)SLOT_GROUPS * 32 * NPARAMS * 8;
+    L.src = o;  o += (size_t)MAXSOURCES * NPARAMS * 8;
+    L.red = o;  o += 16 * 8;
+    L.ints = o; o += 32 * 4;
+    L.idx = o;  o += ((size_t)max_gauss * 2 + 15) & ~(size_t)15;
+    L.total = o;
+    return L;
+}
+
+// ---------------------------------------------------------------------------
+// tile kernel
+// ---------------------------------------------------------------------------
+template <int P>
+__global__ void __launch_bounds__(FP_THREADS, 3)
+tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc *__restrict__ expos,
+            const fp_tile *__restrict__ tiles, const int32_t *__restrict__ order, int64_t n_tiles,
+            const float4 *__restrict__ gfwd, const float4 *__restrict__ gbox,
+            const double *__restrict__ gjac, double *__restrict__ partials, fp_control *ctl,
+            int max_gauss, int flags)
+{
+    constexpr int T = FP_THREADS * P;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const tile_smem L = tile_smem_layout(T, max_gauss);
+    float4 *s_ga = reinterpret_cast<float4 *>(smem + L.ga);
+    float4 *s_gb = reinterpret_cast<float4 *>(smem + L.gb);
+    float4 *s_pix = reinterpret_cast<float4 *>(smem + L.pix);
+    double *s_slot = reinterpret_cast<double *>(smem + L.slot);
+    double *s_src = reinterpret_cast<double *>(smem + L.src);
+    double *s_red = reinterpret_cast<double *>(smem + L.red);
+    int *s_int = reinterpret_cast<int *>(smem + L.ints);          // [0] item, [8..16) warp counts
+    uint16_t *s_idx = reinterpret_cast<uint16_t *>(smem + L.idx);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool nocull = (flags & FP_FLAG_NO_CULL) != 0;
+
+    for (int64_t iter = 0;; ++iter) {
+        if (tid == 0) {
+            const unsigned long long it = (flags & FP_FLAG_STATIC)
+                                              ? (unsigned long long)(blockIdx.x + iter * gridDim.x)
+                                              : atomicAdd(&ctl->queue, 1ULL);
+            s_int[0] = (it < (unsigned long long)n_tiles) ? order[it] : -1;
+        }
+        __syncthreads();
+        const int ti = s_int[0];
+        if (ti < 0) break;
+
+        const fp_tile tl = tiles[ti];
+        const fp_exposure_desc ed = expos[tl.expo];
+        const fp_patch *pt = patches[ed.patch];
+        const int ng = ed.n_gauss, ns = ed.n_sources, n_psf = ed.n_psf;
+        const int npix = tl.n_pix;
+        double *out = partials + tl.partial_offset;
+        if (npix > T || ng > max_gauss || ns > MAXSOURCES) {
+            if (tid == 0) atomicOr(&ctl->status, npix > T ? FP_STATUS_TILE_SIZE : FP_STATUS_GAUSS_COUNT);
+            for (int t = tid; t < 1 + ns * NPARAMS && t < 1 + MAXSOURCES * NPARAMS; t += FP_THREADS)
+                out[t] = 0.0;
+            __syncthreads();
+            continue;
+        }
+
+        // ---- 1. cull (ascending-order compaction of surviving Gaussians) ----
+        const float bx0 = tl.bbox[0], bx1 = tl.bbox[1], by0 = tl.bbox[2], by1 = tl.bbox[3];
+        int gc = 0;
+        for (int g0 = 0; g0 < ng; g0 += FP_THREADS) {
+            const int g = g0 + tid;
+            bool keep = false;
+            if (g < ng) {
+                if (nocull) {
+                    keep = true;
+                } else {
+                    const float4 b = gbox[ed.gauss_offset + g];
+                    keep = (b.y >= bx0) && (b.x <= bx1) && (b.w >= by0) && (b.z <= by1);
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) s_int[8 + warp] = __popc(m);
+            __syncthreads();
+            int off = gc, tot = 0;
+#pragma unroll
+            for (int w = 0; w < FP_WARPS; ++w) {
+                const int cnt = s_int[8 + w];
+                off += (w < warp) ? cnt : 0;
+                tot += cnt;
+            }
+            if (keep) s_idx[off + __popc(m & ((1u << lane) - 1u))] = (uint16_t)g;
+            gc += tot;
+            __syncthreads();
+        }
+
+        // ---- 2. forward: model of P pixels per thread ----
+        const int j0 = tid * P;
+        const int nval = npix - j0;
+        const int gp0 = tl.pix_start + j0;
+        const bool vec = ((((uintptr_t)(pt->xpix + tl.pix_start)) | ((uintptr_t)(pt->ypix + tl.pix_start)) |
+                           ((uintptr_t)(pt->data + tl.pix_start)) | ((uintptr_t)(pt->ierr + tl.pix_start))) &
+                          (4 * P - 1)) == 0;
+        float xs[P], ys[P], ds[P], es[P];
+        if (nval > 0) {
+            load_px<P>(pt->xpix + gp0, vec, nval, xs);
+            load_px<P>(pt->ypix + gp0, vec, nval, ys);
+            load_px<P>(pt->data + gp0, vec, nval, ds);
+            load_px<P>(pt->ierr + gp0, vec, nval, es);
+        } else {
+#pragma unroll
+            for (int k = 0; k < P; ++k) xs[k] = ys[k] = ds[k] = es[k] = 0.f;
+        }
+        double M[P];
+#pragma unroll
+        for (int k = 0; k < P; ++k) M[k] = 0.0;
+
+        for (int c0 = 0; c0 < gc; c0 += FP_CHUNK) {
+            const int cn = min(FP_CHUNK, gc - c0);
+            __syncthreads();
+            for (int i = tid; i < cn; i += FP_THREADS) {
+                const int64_t gi = ed.gauss_offset + s_idx[c0 + i];
+                s_ga[i] = gfwd[2 * gi];
+                s_gb[i] = gfwd[2 * gi + 1];
+            }
+            __syncthreads();
+            if (nval > 0) {
+                for (int r0 = 0; r0 < cn; r0 += FP_RUN) {
+                    const int r1 = min(cn, r0 + FP_RUN);
+                    float m[P];
+#pragma unroll
+                    for (int k = 0; k < P; ++k) m[k] = 0.f;
+#pragma unroll 2
+                    for (int i = r0; i < r1; ++i) {
+                        const float4 A = s_ga[i], B = s_gb[i];
+#pragma unroll
+                        for (int k = 0; k < P; ++k) {
+                            const float dx = xs[k] - A.x, dy = ys[k] - A.y;
+                            const float vx = fmaf(A.z, dx, A.w * dy);
+                            const float vy = fmaf(B.x, dy, A.w * dx);
+                            const float e = fmaf(dy, vy, dx * vx);
+                            const float g = fp_ex2(e);
+                            const float h = fmaf(B.z, fmaf(vx, vx, vy * vy), B.y);
+                            m[k] = (e < FP_CUT_SCALED) ? m[k] : fmaf(g, h, m[k]);
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < P; ++k) M[k] += (double)m[k];
+                }
+            }
+        }
+
+        // residual, chi2 term (f64, the reference's (r^2 - d^2) ierr^2 form), weight
+        float rs[P], ws[P];
+        double chi = 0.0;
+        int nz = 0;
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const bool live = k < nval;
+            const float r = (float)((double)ds[k] - M[k]);
+            rs[k] = r;
+            const float ri = r * es[k], di = ds[k] * es[k];
+            chi += live ? ((double)ri - (double)di) * ((double)ri + (double)di) : 0.0;
+            ws[k] = live ? -2.f * (ri * es[k]) : 0.f;
+            nz += (ws[k] != 0.f) ? 1 : 0;
+        }
+        if (pt->residual != nullptr && nval > 0) {
+            const bool rvec = vec && ((((uintptr_t)(pt->residual + tl.pix_start)) & (4 * P - 1)) == 0);
+            store_px<P>(pt->residual + gp0, rvec, nval, rs);
+        }
+
+        // compact nonzero-weight pixels (ascending) into s_pix; reduce chi2 (fixed tree)
+        int incl = nz;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) chi += __shfl_down_sync(0xffffffffu, chi, o);
+        if (lane == 31) s_int[8 + warp] = incl;
+        if (lane == 0) s_red[warp] = chi;
+        __syncthreads();
+        int off = incl - nz, nzt = 0;
+#pragma unroll
+        for (int w = 0; w < FP_WARPS; ++w) {
+            const int cnt = s_int[8 + w];
+            off += (w < warp) ? cnt : 0;
+            nzt += cnt;
+        }
+#pragma unroll
+        for (int k = 0; k < P; ++k)
+            if (ws[k] != 0.f) s_pix[off++] = make_float4(xs[k], ys[k], ws[k], 0.f);
+        if (tid == 0) {
+            double t = 0.0;
+#pragma unroll
+            for (int w = 0; w < FP_WARPS; ++w) t += s_red[w];
+            s_red[FP_WARPS] = t;
+        }
+        for (int t = tid; t < MAXSOURCES * NPARAMS; t += FP_THREADS) s_src[t] = 0.0;
+
+        // ---- 3. adjoint: one Gaussian per lane, pixels broadcast ----
+        for (int c0 = 0; c0 < gc; c0 += FP_CHUNK) {
+            const int cn = min(FP_CHUNK, gc - c0);
+            __syncthreads();
+            if (gc > FP_CHUNK) {
+                for (int i = tid; i < cn; i += FP_THREADS) {
+                    const int64_t gi = ed.gauss_offset + s_idx[c0 + i];
+                    s_ga[i] = gfwd[2 * gi];
+                    s_gb[i] = gfwd[2 * gi + 1];
+                }
+            }
+            for (int i = tid; i < SLOT_GROUPS * 32 * NPARAMS; i += FP_THREADS) s_slot[i] = 0.0;
+            __syncthreads();
+
+            // the (group of 32 Gaussians) x (pixel) plane, split evenly over the warps;
+            // warp w writes its segment of group g into slot group g + w
+            const int ngrp = (cn + 31) >> 5;
+            const int64_t W = (int64_t)ngrp * nzt;
+            int64_t u = W * warp / FP_WARPS;
+            const int64_t u1 = W * (warp + 1) / FP_WARPS;
+            while (u < u1) {
+                const int grp = (int)(u / nzt);
+                const int p0 = (int)(u - (int64_t)grp * nzt);
+                const int p1 = (int)min((int64_t)nzt, (int64_t)p0 + (u1 - u));
+                const int gl = grp * 32 + lane;
+                const bool valid = gl < cn;
+                const float4 A = valid ? s_ga[gl] : make_float4(0.f, 0.f, 0.f, 0.f);
+                const float4 B = valid ? s_gb[gl] : make_float4(0.f, 0.f, 0.f, 0.f);
+                double mom[12];
+#pragma unroll
+                for (int k = 0; k < 12; ++k) mom[k] = 0.0;
+                adjoint_moments(A, B, s_pix, p0, p1, mom);
+                if (valid) {
+                    const int64_t gi = ed.gauss_offset + s_idx[c0 + gl];
+                    double g7[NPARAMS];
+                    moments_to_grad(gjac + (size_t)FP_JAC * gi, mom, g7);
+                    double *slot = s_slot + ((size_t)(grp + warp) * 32 + lane) * NPARAMS;
+#pragma unroll
+                    for (int k = 0; k < NPARAMS; ++k) slot[k] = g7[k];
+                }
+                u += p1 - p0;
+            }
+            __syncthreads();
+
+            // per-source sums over this chunk, fixed order (Gaussian, then warp)
+            for (int t = tid; t < ns * NPARAMS; t += FP_THREADS) {
+                const int s = t / NPARAMS, k = t - s * NPARAMS;
+                int lo = 0, hi = cn;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if ((int)s_idx[c0 + mid] / n_psf < s) lo = mid + 1; else hi = mid;
+                }
+                int end = lo, hi2 = cn;
+                while (end < hi2) {
+                    const int mid = (end + hi2) >> 1;
+                    if ((int)s_idx[c0 + mid] / n_psf <= s) end = mid + 1; else hi2 = mid;
+                }
+                double acc = 0.0;
+                for (int gl = lo; gl < end; ++gl) {
+                    const int grp = gl >> 5, ln = gl & 31;
+#pragma unroll
+                    for (int w = 0; w < FP_WARPS; ++w)
+                        acc += s_slot[((size_t)(grp + w) * 32 + ln) * NPARAMS + k];
+                }
+                s_src[t] += acc;
+            }
+        }
+        __syncthreads();
+
+        // ---- 4. per-tile partials ----
+        if (tid == 0) out[0] = s_red[FP_WARPS];
+        for (int t = tid; t < ns * NPARAMS; t += FP_THREADS) out[1 + t] = s_src[t];
+        // the next iteration's first barrier orders these reads before any reuse
+    }
+}
+
+// ---------------------------------------------------------------------------
+// reduction over tiles
+// ---------------------------------------------------------------------------
+constexpr int REDUCE_THREADS = 224;
+
+__global__ void __launch_bounds__(REDUCE_THREADS)
+reduce_kernel(const fp_band_desc *__restrict__ bands, const fp_tile *__restrict__ tiles,
+              const double *__restrict__ partials, double *__restrict__ chi2_out,
+              fp_response *__restrict__ resp_out)
+{
+    const fp_band_desc bd = bands[blockIdx.x];
+    const int ns = bd.n_sources;
+    const int stride = 1 + NPARAMS * ns;
+    const int64_t base = (bd.tile_end > bd.tile_begin) ? tiles[bd.tile_begin].partial_offset : 0;
+    const int64_t out = (int64_t)bd.patch * MAXBANDS + bd.band;
+    for (int t = threadIdx.x; t < 1 + MAXSOURCES * NPARAMS; t += REDUCE_THREADS) {
+        double acc = 0.0;
+        if (t < stride)
+            for (int i = 0; i < bd.tile_end - bd.tile_begin; ++i) acc += partials[base + (int64_t)i * stride + t];
+        if (t == 0) chi2_out[out] = acc;
+        else resp_out[out].dchi2_dparam[t - 1] = (float)acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pair census (diagnostic): how many (pixel, Gaussian) pairs the culled tile
+// kernel evaluates, how many lie within the MAX_EXP_ARG cutoff (the pairs that
+// change the result), and how many within-cutoff pairs belong to a Gaussian
+// the cull dropped (must be zero).  Same FP32 exponent as the pixel loops.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+count_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc *__restrict__ expos,
+             const fp_tile *__restrict__ tiles, const float4 *__restrict__ gfwd,
+             const float4 *__restrict__ gbox, unsigned long long *counts)
+{
+    const fp_tile tl = tiles[blockIdx.x];
+    const fp_exposure_desc ed = expos[tl.expo];
+    const fp_patch *pt = patches[ed.patch];
+    unsigned long long inbox = 0, active = 0, bad = 0;
+    for (int j = threadIdx.x; j < tl.n_pix; j += blockDim.x) {
+        const float x = pt->xpix[tl.pix_start + j], y = pt->ypix[tl.pix_start + j];
+        for (int g = 0; g < ed.n_gauss; ++g) {
+            const int64_t gi = ed.gauss_offset + g;
+            const float4 b = gbox[gi];
+            const bool keep = (b.y >= tl.bbox[0]) && (b.x <= tl.bbox[1]) && (b.w >= tl.bbox[2]) && (b.z <= tl.bbox[3]);
+            const float4 A = gfwd[2 * gi], B = gfwd[2 * gi + 1];
+            const float dx = x - A.x, dy = y - A.y;
+            const float vx = fmaf(A.z, dx, A.w * dy);
+            const float vy = fmaf(B.x, dy, A.w * dx);
+            const float e = fmaf(dy, vy, dx * vx);
+            const bool act = !(e < FP_CUT_SCALED);
+            inbox += keep ? 1 : 0;
+            active += act ? 1 : 0;
+            bad += (act && !keep) ? 1 : 0;
+        }
+    }
+    __shared__ unsigned long long s[3][8];
+    for (int o = 16; o > 0; o >>= 1) {
+        inbox += __shfl_down_sync(0xffffffffu, inbox, o);
+        active += __shfl_down_sync(0xffffffffu, active, o);
+        bad += __shfl_down_sync(0xffffffffu, bad, o);
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { s[0][w] = inbox; s[1][w] = active; s[2][w] = bad; }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        unsigned long long t = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += s[threadIdx.x][i];
+        atomicAdd(counts + threadIdx.x, t);
+    }
+}
+
+bool g_attr_set[8][3];
+
+template <int P>
+int launch_tiles(int grid, size_t smem, cudaStream_t st, const fp_patch *const *d_patches,
+                 const fp_exposure_desc *d_expos, const fp_tile *d_tiles, const int32_t *d_order,
+                 int64_t n_tiles, const float4 *gfwd, const float4 *gbox, const double *gjac,
+                 double *partials, fp_control *ctl, int max_gauss, int flags)
+{
+    int dev = 0;
+    if (int rc = fp_check_cuda(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+    const int pi = P == 1 ? 0 : (P == 2 ? 1 : 2);
+    if (dev < 8 && !g_attr_set[dev][pi]) {
+        int optin = 0;
+        if (int rc = fp_check_cuda(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+                                   "cudaDeviceGetAttribute"))
+            return rc;
+        if (int rc = fp_check_cuda(cudaFuncSetAttribute(tile_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        optin),
+                                   "cudaFuncSetAttribute(tile_kernel)"))
+            return rc;
+        g_attr_set[dev][pi] = true;
+    }
+    tile_kernel<P><<<grid, FP_THREADS, smem, st>>>(d_patches, d_expos, d_tiles, d_order, n_tiles, gfwd, gbox,
+                                                    gjac, partials, ctl, max_gauss, flags);
+    return fp_check_cuda(cudaGetLastError(), "tile_kernel launch");
+}
+
+}  // namespace
+
+extern "C" int fp_plan_bbox(const fp_patch *const *d_patches, const fp_exposure_desc *d_expos,
+                            fp_tile *d_tiles, int64_t n_tiles, void *stream)
+{
+    if (!d_patches || !d_expos || !d_tiles || n_tiles < 0)
+        return fp_set_error(FP_ERR_ARGUMENT, "fp_plan_bbox: bad arguments");
+    if (n_tiles == 0) return FP_OK;
+    const int per_block = 8;
+    const int64_t grid = (n_tiles + per_block - 1) / per_block;
+    bbox_kernel<<<(unsigned)grid, 32 * per_block, 0, (cudaStream_t)stream>>>(d_patches, d_expos, d_tiles, n_tiles);
+    return fp_check_cuda(cudaGetLastError(), "bbox_kernel launch");
+}
+
+extern "C" int fp_tile_smem_bytes(int tile_pixels, int64_t max_gauss, int64_t *out)
+{
+    if (!out) return fp_set_error(FP_ERR_ARGUMENT, "fp_tile_smem_bytes: NULL");
+    *out = (int64_t)tile_smem_layout(tile_pixels, (int)max_gauss).total;
+    return FP_OK;
+}
+
+extern "C" int fp_count_pairs(const fp_patch *const *d_patches, const fp_plan_sizes *sizes,
+                              const fp_exposure_desc *d_expos, const fp_tile *d_tiles, const void *d_workspace,
+                              size_t workspace_bytes, unsigned long long *d_counts, void *stream)
+{
+    if (!d_patches || !sizes || !d_expos || !d_tiles || !d_workspace || !d_counts)
+        return fp_set_error(FP_ERR_ARGUMENT, "fp_count_pairs: NULL argument");
+    const fp_workspace_layout L = fp_layout(sizes->n_gauss, sizes->n_partials);
+    if (workspace_bytes < L.total) return fp_set_error(FP_ERR_WORKSPACE, "fp_count_pairs: workspace too small");
+    if (sizes->n_tiles <= 0) return FP_OK;
+    if (sizes->n_tiles > INT32_MAX) return fp_set_error(FP_ERR_LIMITS, "fp_count_pairs: too many tiles");
+    const unsigned char *ws = reinterpret_cast<const unsigned char *>(d_workspace);
+    count_kernel<<<(unsigned)sizes->n_tiles, 256, 0, (cudaStream_t)stream>>>(
+        d_patches, d_expos, d_tiles, reinterpret_cast<const float4 *>(ws + L.gauss_fwd),
+        reinterpret_cast<const float4 *>(ws + L.gauss_box), d_counts);
+    return fp_check_cuda(cudaGetLastError(), "count_kernel launch");
+}
+
+extern "C" int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches, const fp_plan_sizes *sizes,
+                                 const fp_exposure_desc *d_expos, const fp_tile *d_tiles,
+                                 const int32_t *d_order, const fp_band_desc *d_bands,
+                                 const fp_source *d_proposals, double *d_chi2, fp_response *d_response,
+                                 void *d_workspace, size_t workspace_bytes, const fp_launch *launch,
+                                 void *stream)
+{
+    if (!d_patches || n_patches < 1 || !sizes || !d_expos || !d_tiles || !d_order || !d_bands ||
+        !d_proposals || !d_chi2 || !d_response || !d_workspace || !launch)
+        return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch: NULL argument");
+    if (((uintptr_t)d_workspace) & 255)
+        return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch: workspace must be 256-byte aligned");
+    const fp_workspace_layout L = fp_layout(sizes->n_gauss, sizes->n_partials);
+    if (workspace_bytes < L.total)
+        return fp_set_error(FP_ERR_WORKSPACE, "fp_evaluate_batch: workspace %zu B < required %zu B",
+                            workspace_bytes, L.total);
+    const int T = launch->tile_pixels;
+    if (T != 256 && T != 512 && T != 1024)
+        return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch: tile_pixels=%d (supported: 256, 512, 1024)", T);
+    if (sizes->max_gauss > 65535)
+        return fp_set_error(FP_ERR_LIMITS, "fp_evaluate_batch: %lld image Gaussians in one exposure (max 65535)",
+                            (long long)sizes->max_gauss);
+    const size_t smem = tile_smem_layout(T, (int)sizes->max_gauss).total;
+    int dev = 0, optin = 0, nsm = 0;
+    if (int rc = fp_check_cuda(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+    if (int rc = fp_check_cuda(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
+                               "cudaDeviceGetAttribute"))
+        return rc;
+    if (smem > (size_t)optin)
+        return fp_set_error(FP_ERR_LIMITS, "fp_evaluate_batch: tile needs %zu B shared memory (limit %d B)", smem,
+                            optin);
+    if (int rc = fp_sm_count(&nsm)) return rc;
+
+    unsigned char *ws = reinterpret_cast<unsigned char *>(d_workspace);
+    fp_control *ctl = reinterpret_cast<fp_control *>(ws);
+    float4 *gfwd = reinterpret_cast<float4 *>(ws + L.gauss_fwd);
+    float4 *gbox = reinterpret_cast<float4 *>(ws + L.gauss_box);
+    double *gjac = reinterpret_cast<double *>(ws + L.gauss_jac);
+    double *partials = reinterpret_cast<double *>(ws + L.partials);
+    cudaStream_t st = (cudaStream_t)stream;
+
+    const int phases = launch->phases ? launch->phases : (FP_PHASE_SETUP | FP_PHASE_TILES | FP_PHASE_REDUCE);
+    if ((phases & FP_PHASE_SETUP) && sizes->n_exposures > 0) {
+        if (sizes->n_exposures > INT32_MAX) return fp_set_error(FP_ERR_LIMITS, "too many exposures");
+        setup_kernel<<<(unsigned)sizes->n_exposures, 256, 0, st>>>(d_patches, d_expos, d_proposals, gfwd, gbox,
+                                                                   gjac, ctl);
+        if (int rc = fp_check_cuda(cudaGetLastError(), "setup_kernel launch")) return rc;
+    }
+    if ((phases & FP_PHASE_TILES) && sizes->n_tiles > 0) {
+        const int cps = launch->ctas_per_sm > 0 ? launch->ctas_per_sm : 2;
+        const int64_t want = (int64_t)cps * nsm;
+        const int grid = (int)(want < sizes->n_tiles ? want : sizes->n_tiles);
+        int rc;
+        const int mg = (int)sizes->max_gauss;
+        if (T == 256)
+            rc = launch_tiles<1>(grid, smem, st, d_patches, d_expos, d_tiles, d_order, sizes->n_tiles, gfwd, gbox,
+                                 gjac, partials, ctl, mg, launch->flags);
+        else if (T == 512)
+            rc = launch_tiles<2>(grid, smem, st, d_patches, d_expos, d_tiles, d_order, sizes->n_tiles, gfwd, gbox,
+                                 gjac, partials, ctl, mg, launch->flags);
+        else
+            rc = launch_tiles<4>(grid, smem, st, d_patches, d_expos, d_tiles, d_order, sizes->n_tiles, gfwd, gbox,
+                                 gjac, partials, ctl, mg, launch->flags);
+        if (rc) return rc;
+    }
+    if ((phases & FP_PHASE_REDUCE) && sizes->n_band_outputs > 0) {
+        reduce_kernel<<<(unsigned)sizes->n_band_outputs, REDUCE_THREADS, 0, st>>>(d_bands, d_tiles, partials,
+                                                                                  d_chi2, d_response);
+        if (int rc = fp_check_cuda(cudaGetLastError(), "reduce_kernel launch")) return rc;
+    }
+    return FP_OK;
+}

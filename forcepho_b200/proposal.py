@@ -1,0 +1,188 @@
+"""Proposers: the host boundary of the likelihood kernels.
+
+``B200Proposer`` is a drop-in for the reference's ``GPUProposer``
+(forcepho/proposal.py:55-152): ``evaluate_proposal(proposal, patch=None,
+verbose=False, unpack=True)`` takes a ``source_struct_dtype`` array and a patch
+that has been ``send_to_device``-ed, and returns
+
+* ``chi2``        float64[n_bands]
+* ``chi2_derivs`` float32[n_bands, n_sources, 7] (dflux, dra, ddec, dq, dpa,
+  dsersic, drh), a view of the Response records as the reference makes it
+* ``residuals``   list of per-exposure arrays (or the flat array with
+  ``unpack=False``) -- only when ``patch.return_residual``.
+
+It runs the tiled sm_100a kernels through the C ABI (``fp_evaluate_batch`` with
+one patch).  ``PlainProposer`` has the same surface over the one-CTA-per-band
+comparator kernel (``fp_evaluate_proposal_plain``).  ``Proposer`` is an alias
+of ``B200Proposer``, as ``Proposer`` aliases ``GPUProposer`` in the reference.
+"""
+
+import ctypes
+import sys
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .device import Plan, current_stream_ptr, pack_proposals, response_view
+from .kernel_limits import MAXBANDS, MAXRADII, MAXSOURCES, NPARAMS
+from .structs import response_struct_dtype, source_struct_dtype
+
+__all__ = ["ProposerBase", "B200Proposer", "PlainProposer", "Proposer",
+           "source_struct_dtype", "response_struct_dtype", "MAXBANDS", "MAXRADII", "MAXSOURCES", "NPARAMS"]
+
+
+class ProposerBase:
+
+    def evaluate_proposal(self, proposal, **kwargs):
+        raise NotImplementedError
+
+    def unpack_residuals(self, residuals_flat, patch, reshape=False):
+        """Split the flat padded residual into per-exposure arrays; with
+        ``reshape`` drop the padding and reshape to the original stamps
+        (forcepho/proposal.py:38-52)."""
+        residuals = np.split(residuals_flat, np.cumsum(patch.exposure_N)[:-1])
+        if reshape:
+            for e, r in enumerate(residuals):
+                r = r[:patch.original_sizes[e]]
+                residuals[e] = r.reshape(patch.original_shapes[e])
+        return residuals
+
+    @staticmethod
+    def _check_proposal(proposal, patch):
+        p = np.ascontiguousarray(proposal)
+        if p.dtype != source_struct_dtype:
+            p = p.astype(source_struct_dtype)
+        p = p.reshape(-1)
+        if len(p) != int(patch.n_sources):
+            raise ValueError("proposal has %d sources, the patch %d" % (len(p), int(patch.n_sources)))
+        return p
+
+    @staticmethod
+    def _ensure_residual(patch):
+        if patch.return_residual and "residual" not in patch.device_ptrs:
+            patch._alloc_residual()
+            patch.send_patchstruct_to_device()
+
+
+class B200Proposer(ProposerBase):
+    """Evaluate proposals on one device patch with the tiled sm_100a kernels.
+
+    Parameters
+    ----------
+    patch : optional default patch (as in the reference).
+    tile_pixels : pixel-tile size of the work plan (256, 512 or 1024), or None
+        for the autotuned default of the patch's size class.
+    ctas_per_sm : persistent CTAs per SM.
+    flags : extra ``fp_launch`` flags (e.g. ``FLAG_NO_CULL``).
+    """
+
+    def __init__(self, patch=None, tile_pixels=None, ctas_per_sm=3, flags=0):
+        N.load()
+        self.patch = patch
+        self.tile_pixels = tile_pixels
+        self.ctas_per_sm = ctas_per_sm
+        self.flags = flags
+        self._plan = None
+        self._plan_key = None
+        self._pinned_prop = None
+        self._pinned_out = None
+
+    def plan_for(self, patch):
+        key = (id(patch), patch.plan_signature(), self.tile_pixels)
+        if self._plan is None or self._plan_key != key:
+            tp = self.tile_pixels
+            if tp is None:
+                from .autotune import default_tile_pixels
+                tp = default_tile_pixels(patch)
+            self._plan = Plan([patch], tile_pixels=tp)
+            self._plan_key = key
+            self._pinned_prop = torch.zeros(self._plan.proposals.numel(), dtype=torch.uint8).pin_memory()
+            self._pinned_chi2 = torch.zeros((1, MAXBANDS), dtype=torch.float64).pin_memory()
+            self._pinned_resp = torch.zeros((1, MAXBANDS, MAXSOURCES * NPARAMS), dtype=torch.float32).pin_memory()
+        return self._plan
+
+    def evaluate_proposal(self, proposal, patch=None, verbose=False, unpack=True):
+        if patch is None:
+            patch = self.patch
+        prop = self._check_proposal(proposal, patch)
+        self._ensure_residual(patch)
+        plan = self.plan_for(patch)
+        n_bands, n_sources = patch.n_bands, int(patch.n_sources)
+        if verbose:
+            print("Launching tiled evaluation: %d tiles of %d px, %d CTAs/SM"
+                  % (plan.sizes.n_tiles, plan.tile_pixels, self.ctas_per_sm), file=sys.stderr, flush=True)
+        host = pack_proposals([prop], 1)
+        self._pinned_prop.numpy()[:] = host.view(np.uint8).reshape(-1)
+        stream = torch.cuda.current_stream()
+        plan.proposals.copy_(self._pinned_prop, non_blocking=True)
+        plan.evaluate(plan.launch(ctas_per_sm=self.ctas_per_sm, flags=self.flags), stream=stream)
+        self._pinned_chi2.copy_(plan.chi2, non_blocking=True)
+        self._pinned_resp.copy_(plan.response, non_blocking=True)
+        stream.synchronize()
+        chi_out = self._pinned_chi2.numpy()[0, :n_bands].copy()
+        chi_derivs = response_view(self._pinned_resp.numpy()[0], n_bands, n_sources).copy()
+        if patch.return_residual:
+            residuals = patch.retrieve_array("residual")
+            if unpack:
+                residuals = self.unpack_residuals(residuals, patch)
+            return chi_out, chi_derivs, residuals
+        return chi_out, chi_derivs
+
+
+Proposer = B200Proposer
+
+
+class PlainProposer(ProposerBase):
+    """Same surface, evaluated by the port-equivalent kernel: one 1024-thread
+    CTA per band and one launch per patch (the comparator)."""
+
+    def __init__(self, patch=None):
+        self.L = N.load()
+        self.patch = patch
+        self._bufs = None
+
+    def _buffers(self, device):
+        if self._bufs is None:
+            self._bufs = dict(
+                prop=torch.zeros(MAXSOURCES * source_struct_dtype.itemsize, dtype=torch.uint8, device=device),
+                chi2=torch.zeros(MAXBANDS, dtype=torch.float64, device=device),
+                resp=torch.zeros((MAXBANDS, MAXSOURCES * NPARAMS), dtype=torch.float32, device=device),
+                pin_prop=torch.zeros(MAXSOURCES * source_struct_dtype.itemsize, dtype=torch.uint8).pin_memory(),
+                pin_chi2=torch.zeros(MAXBANDS, dtype=torch.float64).pin_memory(),
+                pin_resp=torch.zeros((MAXBANDS, MAXSOURCES * NPARAMS), dtype=torch.float32).pin_memory())
+        return self._bufs
+
+    def launch(self, patch, d_proposal_ptr, d_chi2_ptr, d_resp_ptr, stream=None):
+        """Queue one plain evaluation (device pointers; no host synchronisation)."""
+        N.check(self.L.fp_evaluate_proposal_plain(
+            ctypes.c_void_p(patch.device_patch_ptr), ctypes.c_void_p(d_proposal_ptr), patch.n_bands,
+            patch.max_gauss_per_exposure(), ctypes.c_void_p(d_chi2_ptr), ctypes.c_void_p(d_resp_ptr),
+            current_stream_ptr(stream)), "fp_evaluate_proposal_plain")
+
+    def evaluate_proposal(self, proposal, patch=None, verbose=False, unpack=True):
+        if patch is None:
+            patch = self.patch
+        prop = self._check_proposal(proposal, patch)
+        self._ensure_residual(patch)
+        b = self._buffers(patch.device_patch.device)
+        n_bands, n_sources = patch.n_bands, int(patch.n_sources)
+        host = np.zeros(MAXSOURCES, dtype=source_struct_dtype)
+        host[:len(prop)] = prop
+        b["pin_prop"].numpy()[:] = host.view(np.uint8)
+        stream = torch.cuda.current_stream()
+        b["prop"].copy_(b["pin_prop"], non_blocking=True)
+        if verbose:
+            print("Launching plain kernel with grid (%d,), block 1024" % n_bands, file=sys.stderr, flush=True)
+        self.launch(patch, b["prop"].data_ptr(), b["chi2"].data_ptr(), b["resp"].data_ptr(), stream)
+        b["pin_chi2"].copy_(b["chi2"], non_blocking=True)
+        b["pin_resp"].copy_(b["resp"], non_blocking=True)
+        stream.synchronize()
+        chi_out = b["pin_chi2"].numpy()[:n_bands].copy()
+        chi_derivs = response_view(b["pin_resp"].numpy(), n_bands, n_sources).copy()
+        if patch.return_residual:
+            residuals = patch.retrieve_array("residual")
+            if unpack:
+                residuals = self.unpack_residuals(residuals, patch)
+            return chi_out, chi_derivs, residuals
+        return chi_out, chi_derivs

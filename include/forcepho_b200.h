@@ -1,0 +1,302 @@
+/* forcepho_b200.h -- C ABI of the B200 likelihood library (libforcepho_b200.so).
+ *
+ * The library evaluates forcepho's per-patch likelihood hot path: every active
+ * source's Sersic-as-Gaussian-mixture, convolved with each exposure's PSF
+ * mixture, is rendered into model pixels; the ierr-weighted residuals give
+ *     chi2[band]            = sum_pix (r*ierr - d*ierr) * (r*ierr + d*ierr)   (f64)
+ *     dchi2_dparam[band][s] = d chi2[band] / d(flux, ra, dec, q, pa, sersic, rhalf)_s (f32)
+ * exactly as the reference's EvaluateProposal does
+ * (forcepho/src/compute_gaussians_kernel.cu:212-312, forcepho/src/compute_gaussians_kernel.cc:227-315).
+ *
+ * Conventions
+ *   - All pointers named d_* are device pointers; h_* are host pointers.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *   - Every entry point returns 0 on success, or a negative FP_ERR_* code; nothing is
+ *     printed.  fp_error_string() gives a one-line description of the last error.
+ *   - Entry points never allocate device memory: buffers are owned by the caller
+ *     (the reference's Python patch objects own theirs, forcepho/patches/device_patch.py:265-297).
+ *   - Launches are asynchronous on `stream` and contain no host synchronisation, so a
+ *     sequence of them can be captured into a CUDA graph.
+ */
+#ifndef FORCEPHO_B200_H
+#define FORCEPHO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "forcepho_b200_limits.h"
+
+/* Entry points are the only symbols the shared library exports. */
+#if defined(__GNUC__)
+#define FP_API __attribute__((visibility("default")))
+#else
+#define FP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Boundary records: bit-identical to the reference's structs.               */
+/* ------------------------------------------------------------------------- */
+
+/* One PSF Gaussian, already assigned to a Sersic radius bin: 28 bytes.
+ * Mirrors PSFSourceGaussian (forcepho/src/patch.cc:103-119) and
+ * PSF_DTYPE (forcepho/patches/storage.py:27-28). */
+typedef struct fp_psf_gaussian {
+    float amp;
+    float xcen, ycen;
+    float Cxx, Cyy, Cxy;
+    int32_t sersic_radius_bin;
+} fp_psf_gaussian;
+
+/* Pointers to all pixel and metadata arrays of one patch: 152 bytes.
+ * Mirrors class Patch (forcepho/src/patch.cc:23-100) and PatchBase.pdt
+ * (forcepho/patches/patch.py:45-73).  Array shapes:
+ *   data, ierr, xpix, ypix, residual  f32[n_pix]  (residual may be NULL)
+ *   exposure_start, exposure_N         i32[n_exp]
+ *   band_start, band_N                 i16[n_bands]
+ *   rad2                               f32[n_radii]
+ *   D, CW                              f32[n_exp][n_sources][2][2]
+ *   crpix, crval                       f32[n_exp][n_sources][2]
+ *   G                                  f32[n_exp]
+ *   n_psf_per_source                   i32[n_bands]
+ *   psfgauss                           fp_psf_gaussian[sum_e n_sources*n_psf_per_source[band(e)]]
+ *   psfgauss_start                     i32[n_exp]                                            */
+typedef struct fp_patch {
+    float *data;
+    float *ierr;
+    float *xpix;
+    float *ypix;
+    float *residual;
+    int32_t *exposure_start;
+    int32_t *exposure_N;
+    int16_t *band_start;
+    int16_t *band_N;
+    int32_t n_sources;
+    int32_t n_radii;
+    float *rad2;
+    float *D;
+    float *crpix;
+    float *crval;
+    float *CW;
+    float *G;
+    int32_t *n_psf_per_source;
+    fp_psf_gaussian *psfgauss;
+    int32_t *psfgauss_start;
+} fp_patch;
+
+/* On-sky parameters of one Sersic source: 264 bytes.
+ * Mirrors class Source (forcepho/src/proposal.cu:13-27) and
+ * source_struct_dtype (forcepho/proposal.py:229-240). */
+typedef struct fp_source {
+    float ra, dec;
+    float q, pa;
+    float nsersic, rh;
+    float fluxes[MAXBANDS];
+    float mixture_amplitudes[MAXRADII];
+    float damplitude_drh[MAXRADII];
+    float damplitude_dnsersic[MAXRADII];
+} fp_source;
+
+/* Gradient of one band's chi2: 840 bytes, source-major
+ * (dflux, dra, ddec, dq, dpa, dsersic, drh) per source.
+ * Mirrors class Response (forcepho/src/proposal.cu:33-39) and
+ * response_struct_dtype (forcepho/proposal.py:243-244). */
+typedef struct fp_response {
+    float dchi2_dparam[MAXSOURCES * NPARAMS];
+} fp_response;
+
+/* ------------------------------------------------------------------------- */
+/* Error handling                                                            */
+/* ------------------------------------------------------------------------- */
+
+#define FP_OK               0
+#define FP_ERR_ARGUMENT    -1   /* bad argument (NULL, out-of-range count, misalignment) */
+#define FP_ERR_LIMITS      -2   /* a count exceeds MAXSOURCES/MAXBANDS/shared memory */
+#define FP_ERR_CUDA        -3   /* a CUDA runtime call failed */
+#define FP_ERR_WORKSPACE   -4   /* workspace smaller than required */
+#define FP_ERR_DEVICE      -5   /* a kernel reported an inconsistency in its status word */
+
+/* One-line description of the most recent error on the calling thread. */
+FP_API const char *fp_error_string(void);
+
+/* Library version as an integer (major*10000 + minor*100 + patch). */
+FP_API int fp_version(void);
+
+/* Size checks a binding can run at load time: returns sizeof of the four
+ * boundary records in out[0..3] (patch, source, response, psf gaussian). */
+FP_API int fp_struct_sizes(int32_t out[4]);
+
+/* ------------------------------------------------------------------------- */
+/* Plain path: one patch per launch, port-equivalent decomposition.          */
+/* ------------------------------------------------------------------------- */
+
+/* Evaluate one proposal on one patch with the reference's decomposition:
+ * one 1024-thread CTA per band, the band's image-Gaussian table in shared
+ * memory, one pixel per thread, warp-shuffle + shared-atomic accumulation.
+ * This is the comparator for the batched path.
+ *
+ * Replaces the pycuda launch in GPUProposer.evaluate_proposal
+ * (forcepho/proposal.py:133-136) of EvaluateProposal
+ * (forcepho/src/compute_gaussians_kernel.cu:212-312).
+ *
+ *   d_patch                device fp_patch
+ *   d_proposal             device fp_source[n_sources]
+ *   n_bands                grid size (number of bands in the patch)
+ *   max_gauss_per_exposure n_sources * max_b n_psf_per_source[b]; sizes shared memory
+ *   d_chi2                 device f64[n_bands]
+ *   d_response             device fp_response[n_bands]
+ */
+FP_API int fp_evaluate_proposal_plain(const fp_patch *d_patch, const fp_source *d_proposal,
+                               int n_bands, int max_gauss_per_exposure,
+                               double *d_chi2, fp_response *d_response, void *stream);
+
+/* ------------------------------------------------------------------------- */
+/* Tiled / batched path.                                                     */
+/* ------------------------------------------------------------------------- */
+/* A "plan" covers one or many patches whose pixel layout is fixed.  It splits
+ * every exposure into pixel tiles (the work items of one persistent launch) and
+ * lays out the workspace.  Planning runs on the host from the host copies of
+ * each patch's index arrays; the caller copies the three host tables the plan
+ * fills to device memory and passes them to fp_evaluate_batch. */
+
+/* Host-side shape of one patch (pointers are host copies of the index arrays). */
+typedef struct fp_patch_shape {
+    int32_t n_bands;
+    int32_t n_exposures;
+    int32_t n_sources;
+    int32_t n_pix;                      /* total (padded) pixels */
+    const int32_t *exposure_start;      /* [n_exposures] */
+    const int32_t *exposure_N;          /* [n_exposures] */
+    const int16_t *band_start;          /* [n_bands] */
+    const int16_t *band_N;              /* [n_bands] */
+    const int32_t *n_psf_per_source;    /* [n_bands] */
+} fp_patch_shape;
+
+/* Device descriptor of one exposure of one patch (planner output). */
+typedef struct fp_exposure_desc {
+    int64_t gauss_offset;   /* first image Gaussian of this exposure in the Gaussian table */
+    int32_t patch;          /* patch index in the plan */
+    int32_t exposure;       /* exposure index within the patch */
+    int32_t band;           /* band index within the patch */
+    int32_t n_gauss;        /* n_sources * n_psf_per_source[band] */
+    int32_t n_psf;          /* n_psf_per_source[band] */
+    int32_t n_sources;
+} fp_exposure_desc;        /* 32 bytes */
+
+/* Device work item: one tile of consecutive pixels of one exposure. */
+typedef struct fp_tile {
+    int64_t partial_offset; /* first double of this tile's partials in the workspace */
+    int32_t expo;           /* index into the plan's fp_exposure_desc table */
+    int32_t pix_start;      /* first pixel (index into the patch's pixel arrays) */
+    int32_t n_pix;          /* pixels in the tile (<= tile_pixels) */
+    int32_t pad;
+    float bbox[4];          /* xmin, xmax, ymin, ymax of the tile's pixels (device-filled) */
+} fp_tile;                 /* 40 bytes */
+
+/* Device descriptor of one (patch, band) output. */
+typedef struct fp_band_desc {
+    int32_t patch;          /* patch index in the plan */
+    int32_t band;           /* band index within the patch */
+    int32_t tile_begin;     /* tiles [tile_begin, tile_end) in canonical order hold this band */
+    int32_t tile_end;
+    int32_t n_sources;
+    int32_t pad;
+} fp_band_desc;            /* 24 bytes */
+
+/* Sizes of a plan (filled by fp_plan_count). */
+typedef struct fp_plan_sizes {
+    int64_t n_exposures;    /* fp_exposure_desc entries */
+    int64_t n_tiles;        /* fp_tile entries */
+    int64_t n_band_outputs; /* fp_band_desc entries */
+    int64_t n_gauss;        /* image Gaussians per evaluation, all exposures */
+    int64_t n_pairs;        /* (pixel, image Gaussian) pairs per evaluation */
+    int64_t n_partials;     /* doubles of per-tile partial sums */
+    int64_t max_gauss;      /* largest image-Gaussian count of one exposure */
+    int64_t workspace_bytes;/* device workspace fp_evaluate_batch needs */
+} fp_plan_sizes;
+
+/* Count the plan of `n_patches` patches split into tiles of `tile_pixels`
+ * pixels (a multiple of 32, at most 4096). */
+FP_API int fp_plan_count(const fp_patch_shape *h_shapes, int n_patches, int tile_pixels,
+                  fp_plan_sizes *out);
+
+/* Fill the host tables of a plan (sizes from fp_plan_count).  Tiles are emitted
+ * in canonical order (patch, band, exposure, pixel); h_order receives an
+ * execution order (largest estimated work first) of length n_tiles. */
+FP_API int fp_plan_fill(const fp_patch_shape *h_shapes, int n_patches, int tile_pixels,
+                 fp_exposure_desc *h_expos, fp_tile *h_tiles, fp_band_desc *h_bands,
+                 int32_t *h_order);
+
+/* One-time device pass after the tables are uploaded: computes each tile's
+ * pixel bounding box from the patch's xpix/ypix.  d_patches: device array of
+ * n_patches device fp_patch pointers. */
+FP_API int fp_plan_bbox(const fp_patch *const *d_patches, const fp_exposure_desc *d_expos,
+                 fp_tile *d_tiles, int64_t n_tiles, void *stream);
+
+/* Launch parameters of the batched evaluation (chosen by the autotuner). */
+typedef struct fp_launch {
+    int32_t tile_pixels;    /* pixels per tile: 256, 512 or 1024; must equal the plan's */
+    int32_t ctas_per_sm;    /* persistent CTAs per SM (grid = ctas_per_sm * SM count) */
+    int32_t flags;          /* FP_FLAG_* */
+    int32_t phases;         /* FP_PHASE_* bits to run; 0 = all three */
+} fp_launch;
+
+#define FP_FLAG_NO_CULL     1   /* evaluate every (tile, Gaussian) pair (no bounding-box culling) */
+#define FP_FLAG_STATIC      2   /* static round-robin tile assignment instead of an atomic queue */
+
+#define FP_PHASE_SETUP      1   /* image-Gaussian tables (must precede the tile phase) */
+#define FP_PHASE_TILES      2   /* the persistent tile kernel */
+#define FP_PHASE_REDUCE     4   /* fixed-order reduction into chi2 / response */
+
+/* Shared memory one tile CTA needs for a tile size and largest exposure
+ * Gaussian count (for occupancy planning). */
+FP_API int fp_tile_smem_bytes(int tile_pixels, int64_t max_gauss, int64_t *out);
+
+/* Evaluate one proposal per patch for every patch of a plan in one pass
+ * (Gaussian setup, one persistent tile launch, fixed-order reduction).
+ *   d_patches     device array [n_patches] of device fp_patch pointers
+ *   sizes         the plan's sizes (host struct from fp_plan_count)
+ *   d_expos, d_tiles, d_order, d_bands   the plan's tables (device copies;
+ *                 d_tiles after fp_plan_bbox)
+ *   d_proposals   device fp_source[n_patches][MAXSOURCES] (rows >= n_sources unused)
+ *   d_chi2        device f64[n_patches][MAXBANDS]        (bands >= n_bands untouched)
+ *   d_response    device fp_response[n_patches][MAXBANDS]
+ *   d_workspace   device buffer of at least sizes->workspace_bytes, 256-byte aligned
+ * Replaces, for many patches at once, the per-patch GPUProposer.evaluate_proposal
+ * launch (forcepho/proposal.py:96-152).  Results are bitwise reproducible for
+ * fixed inputs and launch parameters. */
+FP_API int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches, const fp_plan_sizes *sizes,
+                      const fp_exposure_desc *d_expos, const fp_tile *d_tiles,
+                      const int32_t *d_order, const fp_band_desc *d_bands,
+                      const fp_source *d_proposals, double *d_chi2, fp_response *d_response,
+                      void *d_workspace, size_t workspace_bytes, const fp_launch *launch,
+                      void *stream);
+
+/* Pair census of a plan (diagnostic; needs the Gaussian tables of a prior
+ * fp_evaluate_batch in the same workspace).  Adds to d_counts[0..2] (zero them
+ * first): [0] (pixel, Gaussian) pairs the culled tile kernel evaluates,
+ * [1] pairs within the MAX_EXP_ARG cutoff, [2] within-cutoff pairs of Gaussians
+ * the cull dropped (0 unless culling is wrong).  No reference counterpart. */
+FP_API int fp_count_pairs(const fp_patch *const *d_patches, const fp_plan_sizes *sizes,
+                          const fp_exposure_desc *d_expos, const fp_tile *d_tiles,
+                          const void *d_workspace, size_t workspace_bytes,
+                          unsigned long long *d_counts, void *stream);
+
+/* Measure FP32 FMA throughput (TFLOP/s, FMA = 2 flops) and SFU ex2
+ * throughput (results/s) of the current device with two short kernels; the
+ * roofline denominators of this path.  d_scratch: 256 floats.  Synchronises
+ * `stream`.  No reference counterpart (measurement utility). */
+FP_API int fp_measure_peaks(float *d_scratch, double *fp32_tflops, double *ex2_per_s, void *stream);
+
+/* Read and clear the device status word written by the batched kernels
+ * (0 = no inconsistency seen).  Synchronises `stream`. */
+FP_API int fp_read_status(void *d_workspace, int32_t *status_out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FORCEPHO_B200_H */

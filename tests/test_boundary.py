@@ -1,0 +1,131 @@
+"""The drop-in boundary on CPU: record layouts, the C-ABI library's exports,
+the host planner and host-side validation.  No CUDA device needed."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from forcepho_b200 import _native as N
+from forcepho_b200 import kernel_limits as K
+from forcepho_b200 import structs
+from forcepho_b200 import synthetic as S
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "forcepho_b200.h")
+
+
+def test_limits_match_reference_values():
+    # forcepho/src/kernel_limits.h:5-26
+    assert (K.MAXBANDS, K.MAXSOURCES, K.NPARAMS, K.MAX_EXP_ARG, K.MAXRADII) == (30, 30, 7, 36.0, 10)
+
+
+def test_struct_sizes():
+    assert structs.patch_struct_dtype.itemsize == 152
+    assert structs.source_struct_dtype.itemsize == 264
+    assert structs.response_struct_dtype.itemsize == 840
+    assert structs.psf_dtype.itemsize == 28
+    # field offsets of the patch struct (forcepho/src/patch.cc:23-100)
+    off = {n: structs.patch_struct_dtype.fields[n][1] for n in structs.patch_struct_dtype.names}
+    assert off["n_sources"] == 72 and off["n_radii"] == 76 and off["rad2"] == 80 and off["psfgauss_start"] == 144
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"FP_API[^;(]*?\b(fp_\w+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = N.load()
+    syms = declared_symbols()
+    assert len(syms) >= 9
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(syms) == set(N.SIGNATURES), "binding signatures and header disagree"
+
+
+def test_struct_sizes_reported_by_library():
+    L = N.load()
+    out = np.zeros(4, np.int32)
+    assert L.fp_struct_sizes(out.ctypes.data) == 0
+    assert list(out) == [152, 264, 840, 28]
+
+
+def plan(patches, tile):
+    L = N.load()
+    shapes = [N.patch_shape(p) for p in patches]
+    arr = (N.PatchShape * len(shapes))(*shapes)
+    sz = N.PlanSizes()
+    rc = L.fp_plan_count(ctypes.addressof(arr), len(shapes), tile, ctypes.byref(sz))
+    if rc:
+        return rc, None
+    ex = np.zeros(sz.n_exposures, N.exposure_desc_dtype)
+    ti = np.zeros(sz.n_tiles, N.tile_dtype)
+    bd = np.zeros(sz.n_band_outputs, N.band_desc_dtype)
+    od = np.zeros(sz.n_tiles, np.int32)
+    N.check(L.fp_plan_fill(ctypes.addressof(arr), len(shapes), tile, ex.ctypes.data, ti.ctypes.data,
+                           bd.ctypes.data, od.ctypes.data), "fill")
+    return 0, (sz, ex, ti, bd, od)
+
+
+@pytest.mark.parametrize("tile", [256, 512, 1024])
+def test_planner_tables(tile):
+    patches = S.config_batched(seed=7, n_patches=6)
+    rc, (sz, ex, ti, bd, od) = plan(patches, tile)
+    assert rc == 0
+    assert sz.n_pairs == sum(p.n_pairs() for p in patches)
+    assert sz.n_exposures == sum(p.n_exp for p in patches)
+    assert sz.n_band_outputs == sum(p.n_bands for p in patches)
+    # every pixel of every exposure is covered exactly once, in canonical order
+    k = 0
+    for pi, p in enumerate(patches):
+        ns = int(p.n_sources)
+        for b in range(p.n_bands):
+            e0, ne = int(p.band_start[b]), int(p.band_N[b])
+            row = bd[[i for i in range(len(bd)) if bd["patch"][i] == pi and bd["band"][i] == b][0]]
+            assert row["tile_begin"] == k
+            for e in range(e0, e0 + ne):
+                covered = 0
+                while covered < p.exposure_N[e]:
+                    t = ti[k]
+                    assert ex[t["expo"]]["patch"] == pi and ex[t["expo"]]["exposure"] == e
+                    assert t["pix_start"] == p.exposure_start[e] + covered
+                    assert 0 < t["n_pix"] <= tile
+                    covered += t["n_pix"]
+                    k += 1
+            assert row["tile_end"] == k
+            assert row["n_sources"] == ns
+    assert k == sz.n_tiles
+    # partial offsets are dense with the per-patch stride
+    stride = np.array([1 + 7 * ex[t["expo"]]["n_sources"] for t in ti])
+    assert np.array_equal(ti["partial_offset"], np.concatenate([[0], np.cumsum(stride)[:-1]]))
+    assert sz.n_partials == stride.sum()
+    # execution order: a permutation, largest work first
+    assert sorted(od.tolist()) == list(range(sz.n_tiles))
+    work = ti["n_pix"][od].astype(np.int64) * ex[ti["expo"][od]]["n_gauss"]
+    assert np.all(np.diff(work) <= 0)
+
+
+def test_planner_rejects_bad_shapes():
+    p = S.config_small(seed=1)
+    assert plan([p], 100)[0] == N.FP_ERR_ARGUMENT          # not a multiple of 32
+    bad = S.config_small(seed=1)
+    bad.exposure_N = bad.exposure_N + 64          # past the end of the pixel arrays
+    assert plan([bad], 256)[0] == N.FP_ERR_ARGUMENT
+    assert "outside" in N.load().fp_error_string().decode()
+
+
+def test_validate_rejects_inconsistent_patch():
+    p = S.config_multiband(seed=2, n_sources=3, n_bands=2, exp_per_band=2, size=40)
+    assert p.validate()
+    q = S.config_multiband(seed=2, n_sources=3, n_bands=2, exp_per_band=2, size=40)
+    q.band_N = q.band_N.copy()
+    q.band_N[0] = 3
+    with pytest.raises(ValueError):
+        q.validate()
+    r = S.config_multiband(seed=2, n_sources=3, n_bands=2, exp_per_band=2, size=40)
+    r.psfgauss = r.psfgauss.copy()
+    r.psfgauss["sersic_bin"][0] = 12
+    with pytest.raises(ValueError):
+        r.validate()
