@@ -446,7 +446,7 @@ def run_ours(args):
         c_b, g_b = bres[i]
         c_p = pc[i, :p.n_bands]
         g_p = pr[i].reshape(30, 30, 7)[:p.n_bands, :int(p.n_sources)]
-        scale = np.sum(np.abs(c_b)) + 1.0
+        scale = float(np.sum((p.data.astype(np.float64) * p.ierr) ** 2)) + 1e-300
         worst_c = max(worst_c, float(np.max(np.abs(c_b - c_p)) / scale))
         den = np.linalg.norm(g_b) + 1e-30
         worst_g = max(worst_g, float(np.linalg.norm(g_b - g_p) / den))

@@ -32,6 +32,21 @@ class Launch(ctypes.Structure):
     _fields_ = [("tile_pixels", c_i32), ("ctas_per_sm", c_i32), ("flags", c_i32), ("phases", c_i32)]
 
 
+class SplineTable(ctypes.Structure):
+    _fields_ = [("n_radii", c_i32), ("nx", c_i32), ("ny", c_i32), ("kx", c_i32), ("ky", c_i32), ("pad", c_i32),
+                ("tx", c_vp), ("ty", c_vp), ("coef", c_vp)]
+
+
+class HMCState(ctypes.Structure):
+    _fields_ = [("n_params", c_i64), ("z", c_vp), ("p", c_vp), ("grad", c_vp), ("z0", c_vp), ("grad0", c_vp),
+                ("inv_mass", c_vp), ("eps", c_vp), ("lnp", c_vp), ("lnp0", c_vp), ("h0", c_vp),
+                ("energy_error", c_vp), ("accepted", c_vp), ("normals", c_vp), ("uniforms", c_vp),
+                ("traj", c_vp)]
+
+
+HMC_BEGIN, HMC_STEP, HMC_END = 0, 1, 2
+hmc_patch_dtype = np.dtype([("param_offset", np.int64), ("n_sources", np.int32), ("n_bands", np.int32)])
+
 FLAG_NO_CULL = 1
 FLAG_STATIC = 2
 PHASE_SETUP, PHASE_TILES, PHASE_REDUCE = 1, 2, 4
@@ -63,6 +78,10 @@ SIGNATURES = {
                                          c_vp, c_vp, c_vp, c_vp, c_vp, c_sz, ctypes.POINTER(Launch), c_vp]),
     "fp_read_status": (ctypes.c_int, [c_vp, ctypes.POINTER(c_i32), c_vp]),
     "fp_count_pairs": (ctypes.c_int, [c_vp, ctypes.POINTER(PlanSizes), c_vp, c_vp, c_vp, c_sz, c_vp, c_vp]),
+    "fp_hmc_prepare": (ctypes.c_int, [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "fp_hmc_lnprob": (ctypes.c_int, [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, ctypes.c_int, ctypes.c_int,
+                                     c_vp, c_vp, c_vp]),
+    "fp_hmc_leapfrog": (ctypes.c_int, [c_vp, ctypes.c_int, c_vp, ctypes.c_int, c_vp]),
     "fp_measure_peaks": (ctypes.c_int, [c_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                         c_vp]),
 }

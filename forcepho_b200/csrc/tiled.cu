@@ -40,7 +40,6 @@ setup_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc
              const fp_source *__restrict__ proposals, float4 *__restrict__ gfwd,
              float4 *__restrict__ gbox, double *__restrict__ gjac, fp_control *ctl)
 {
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->queue = 0ULL;   // work queue of tile_kernel
     const fp_exposure_desc ed = expos[blockIdx.x];
     const fp_patch *pt = patches[ed.patch];
     if (ed.n_sources > MAXSOURCES || pt->n_sources != ed.n_sources) {
@@ -382,11 +381,13 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
 #pragma unroll
         for (int k = 0; k < P; ++k) {
             const bool live = k < nval;
-            const float r = (float)((double)ds[k] - M[k]);
+            const double rd = (double)ds[k] - M[k];
+            const float r = (float)rd;
             rs[k] = r;
-            const float ri = r * es[k], di = ds[k] * es[k];
-            chi += live ? ((double)ri - (double)di) * ((double)ri + (double)di) : 0.0;
-            ws[k] = live ? -2.f * (ri * es[k]) : 0.f;
+            // chi2 term (r ierr - d ierr)(r ierr + d ierr) from the FP64 residual
+            const double rid = rd * (double)es[k], did = (double)ds[k] * (double)es[k];
+            chi += live ? (rid - did) * (rid + did) : 0.0;
+            ws[k] = live ? -2.f * ((r * es[k]) * es[k]) : 0.f;
             nz += (ws[k] != 0.f) ? 1 : 0;
         }
         if (pt->residual != nullptr && nval > 0) {
@@ -484,9 +485,14 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
                 double acc = 0.0;
                 for (int gl = lo; gl < end; ++gl) {
                     const int grp = gl >> 5, ln = gl & 31;
+                    // slot group grp + w holds warp w's segment of group grp only if
+                    // warp w's share [W w/8, W (w+1)/8) of the plane meets this group's row
+                    const int64_t r0 = (int64_t)grp * nzt, r1 = r0 + nzt;
 #pragma unroll
-                    for (int w = 0; w < FP_WARPS; ++w)
-                        acc += s_slot[((size_t)(grp + w) * 32 + ln) * NPARAMS + k];
+                    for (int w = 0; w < FP_WARPS; ++w) {
+                        const int64_t a = W * w / FP_WARPS, b = W * (w + 1) / FP_WARPS;
+                        if (a < b && a < r1 && b > r0) acc += s_slot[((size_t)(grp + w) * 32 + ln) * NPARAMS + k];
+                    }
                 }
                 s_src[t] += acc;
             }
@@ -689,6 +695,9 @@ extern "C" int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches
         const int cps = launch->ctas_per_sm > 0 ? launch->ctas_per_sm : 2;
         const int64_t want = (int64_t)cps * nsm;
         const int grid = (int)(want < sizes->n_tiles ? want : sizes->n_tiles);
+        // the persistent CTAs pop tiles from this counter
+        if (int rc = fp_check_cuda(cudaMemsetAsync(&ctl->queue, 0, sizeof(ctl->queue), st), "queue reset"))
+            return rc;
         int rc;
         const int mg = (int)sizes->max_gauss;
         if (T == 256)

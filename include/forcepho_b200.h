@@ -291,6 +291,76 @@ FP_API int fp_count_pairs(const fp_patch *const *d_patches, const fp_plan_sizes 
  * `stream`.  No reference counterpart (measurement utility). */
 FP_API int fp_measure_peaks(float *d_scratch, double *fp32_tflops, double *ex2_per_s, void *stream);
 
+/* ------------------------------------------------------------------------- */
+/* Device-resident HMC around the batched likelihood.                        */
+/* ------------------------------------------------------------------------- */
+/* The host-side steps the reference runs per likelihood call -- the sigmoid
+ * parameter transform (forcepho/model.py:596-637), the proposal with spline
+ * amplitudes (forcepho/sources.py:607-681), lnp and stack_grad
+ * (forcepho/model.py:302-387) -- as device launches, plus fixed-length HMC
+ * leapfrog / Metropolis updates standing in for the NUTS sampler of
+ * forcepho/fitting.py:254-341.  All scalars live in device memory, so the
+ * launches of a trajectory can be captured into one CUDA graph. */
+
+/* Tensor-product B-spline tables of the Sersic mixture amplitudes
+ * A_r(sersic, rhalf), r < n_radii (scipy RectBivariateSpline knots and
+ * coefficients; x = sersic, y = rhalf).  Pointers are device pointers. */
+typedef struct fp_spline_table {
+    int32_t n_radii;
+    int32_t nx, ny;          /* knot counts */
+    int32_t kx, ky;          /* degrees */
+    int32_t pad;
+    const double *tx;        /* [nx] */
+    const double *ty;        /* [ny] */
+    const double *coef;      /* [n_radii][(nx-kx-1)*(ny-ky-1)], x-major */
+} fp_spline_table;
+
+/* Parameter layout of one patch: per active source
+ * [flux_1..flux_nb, ra, dec, q, pa, sersic, rhalf] (forcepho/sources.py:559-605). */
+typedef struct fp_hmc_patch {
+    int64_t param_offset;    /* first parameter of the patch in the flat state vectors */
+    int32_t n_sources;
+    int32_t n_bands;
+} fp_hmc_patch;              /* 16 bytes */
+
+/* theta = lower + (upper - lower) sigmoid(z) (theta = z when d_lower is NULL),
+ * the proposal records d_proposals[n_patches][MAXSOURCES] from theta (spline
+ * amplitudes and their sersic / rhalf derivatives evaluated on the device), and
+ * the transform's diagonal Jacobian d_jac = dtheta/dz. */
+FP_API int fp_hmc_prepare(const fp_hmc_patch *d_hp, int n_patches, const double *d_z,
+                          const double *d_lower, const double *d_upper, const fp_spline_table *tab,
+                          fp_source *d_proposals, double *d_theta, double *d_jac, void *stream);
+
+/* lnp[p] = -1/2 sum_b chi2[p][b] (+ log|dtheta/dz| when transformed && sampling)
+ * and grad = dlnp/dz = (-1/2 stack_grad(dchi2)) dtheta/dz (+ 1 - 2 sigmoid(z)),
+ * from the outputs of fp_evaluate_batch. */
+FP_API int fp_hmc_lnprob(const fp_hmc_patch *d_hp, int n_patches, const double *d_z, const double *d_jac,
+                         const double *d_chi2, const fp_response *d_response, int transformed,
+                         int sampling, double *d_lnp, double *d_grad, void *stream);
+
+/* State of HMC over all patches (device pointers). */
+typedef struct fp_hmc_state {
+    int64_t n_params;        /* parameters over all patches */
+    double *z, *p, *grad;    /* [n_params] position (unconstrained), momentum, dlnp/dz */
+    double *z0, *grad0;      /* [n_params] saved at the start of a trajectory */
+    const double *inv_mass;  /* [n_params] diagonal inverse mass matrix */
+    const double *eps;       /* [n_patches] leapfrog step sizes */
+    double *lnp, *lnp0, *h0; /* [n_patches] current / saved lnp, initial energy */
+    double *energy_error;    /* [n_patches] H0 - H1 of the last trajectory */
+    int32_t *accepted;       /* [n_patches] accepted trajectories */
+    const double *normals;   /* [n_traj][n_params] standard normal draws */
+    const double *uniforms;  /* [n_traj][n_patches] uniform draws */
+    int64_t *traj;           /* current trajectory index (advanced by FP_HMC_END) */
+} fp_hmc_state;
+
+#define FP_HMC_BEGIN 0   /* draw momentum, save state, half kick, drift */
+#define FP_HMC_STEP  1   /* full kick, drift (between two gradient evaluations) */
+#define FP_HMC_END   2   /* half kick, Metropolis accept/restore, advance traj */
+
+/* One stage of a leapfrog trajectory (see FP_HMC_*). */
+FP_API int fp_hmc_leapfrog(const fp_hmc_patch *d_hp, int n_patches, const fp_hmc_state *state, int stage,
+                           void *stream);
+
 /* Read and clear the device status word written by the batched kernels
  * (0 = no inconsistency seen).  Synchronises `stream`. */
 FP_API int fp_read_status(void *d_workspace, int32_t *status_out, void *stream);
