@@ -41,7 +41,7 @@ class HMCState(ctypes.Structure):
     _fields_ = [("n_params", c_i64), ("z", c_vp), ("p", c_vp), ("grad", c_vp), ("z0", c_vp), ("grad0", c_vp),
                 ("inv_mass", c_vp), ("eps", c_vp), ("lnp", c_vp), ("lnp0", c_vp), ("h0", c_vp),
                 ("energy_error", c_vp), ("accepted", c_vp), ("normals", c_vp), ("uniforms", c_vp),
-                ("traj", c_vp)]
+                ("traj", c_vp), ("n_traj", c_i64)]
 
 
 HMC_BEGIN, HMC_STEP, HMC_END = 0, 1, 2

@@ -202,7 +202,7 @@ begin_kernel(const fp_hmc_patch *__restrict__ hp, const fp_hmc_state st)
     const int p = blockIdx.x;
     const fp_hmc_patch P = hp[p];
     const int n = P.n_sources * (P.n_bands + NPARAMS - 1);
-    const int64_t traj = *st.traj;
+    const int64_t traj = *st.traj % st.n_traj;
     const double eps = st.eps[p];
     double kin = 0.0;
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
@@ -249,7 +249,7 @@ end_kernel(const fp_hmc_patch *__restrict__ hp, int n_patches, const fp_hmc_stat
     const int p = blockIdx.x;
     const fp_hmc_patch P = hp[p];
     const int n = P.n_sources * (P.n_bands + NPARAMS - 1);
-    const int64_t traj = *st.traj;
+    const int64_t traj = *st.traj % st.n_traj;
     const double eps = st.eps[p];
     double kin = 0.0;
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
@@ -314,7 +314,7 @@ extern "C" int fp_hmc_lnprob(const fp_hmc_patch *d_hp, int n_patches, const doub
 extern "C" int fp_hmc_leapfrog(const fp_hmc_patch *d_hp, int n_patches, const fp_hmc_state *state, int stage,
                                void *stream)
 {
-    if (!d_hp || n_patches < 1 || !state)
+    if (!d_hp || n_patches < 1 || !state || state->n_traj < 1)
         return fp_set_error(FP_ERR_ARGUMENT, "fp_hmc_leapfrog: bad arguments");
     cudaStream_t st = (cudaStream_t)stream;
     if (stage == FP_HMC_BEGIN) {

@@ -718,3 +718,4 @@ extern "C" int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches
     }
     return FP_OK;
 }
+

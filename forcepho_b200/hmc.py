@@ -135,7 +135,8 @@ class DeviceHMC:
                                 self.z0.data_ptr(), self.grad0.data_ptr(), self.inv_mass.data_ptr(),
                                 self.eps.data_ptr(), self.lnp.data_ptr(), self.lnp0.data_ptr(),
                                 self.h0.data_ptr(), self.energy_error.data_ptr(), self.accepted.data_ptr(),
-                                self.normals.data_ptr(), self.uniforms.data_ptr(), self.traj.data_ptr())
+                                self.normals.data_ptr(), self.uniforms.data_ptr(), self.traj.data_ptr(),
+                                self.max_traj)
         self.graph = None
         self.n_evals = 0
 
@@ -213,7 +214,10 @@ class DeviceHMC:
             acc += (self.grad - g0) * v / h
         self.z.copy_(z)
         self.gradient()
-        curv = torch.clamp(-acc / n_probe, min=floor)
+        curv = -acc / n_probe
+        pos = curv[curv > 0]
+        rel = float(pos.median()) * 1e-2 if pos.numel() else 1.0
+        curv = torch.clamp(curv, min=max(floor, rel))
         self.inv_mass.copy_(1.0 / curv)
         torch.cuda.synchronize()
         return self.inv_mass

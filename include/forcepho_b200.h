@@ -351,6 +351,7 @@ typedef struct fp_hmc_state {
     const double *normals;   /* [n_traj][n_params] standard normal draws */
     const double *uniforms;  /* [n_traj][n_patches] uniform draws */
     int64_t *traj;           /* current trajectory index (advanced by FP_HMC_END) */
+    int64_t n_traj;          /* rows of normals/uniforms; trajectory t uses row t % n_traj */
 } fp_hmc_state;
 
 #define FP_HMC_BEGIN 0   /* draw momentum, save state, half kick, drift */
