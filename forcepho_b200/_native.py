@@ -45,6 +45,7 @@ class HMCState(ctypes.Structure):
 
 
 HMC_BEGIN, HMC_STEP, HMC_END = 0, 1, 2
+NOALLOC_WORKSPACE_BYTES = 32 << 20
 hmc_patch_dtype = np.dtype([("param_offset", np.int64), ("n_sources", np.int32), ("n_bands", np.int32)])
 
 FLAG_NO_CULL = 1
@@ -76,6 +77,8 @@ SIGNATURES = {
     "fp_tile_smem_bytes": (ctypes.c_int, [ctypes.c_int, c_i64, ctypes.POINTER(c_i64)]),
     "fp_evaluate_batch": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.POINTER(PlanSizes), c_vp, c_vp, c_vp,
                                          c_vp, c_vp, c_vp, c_vp, c_vp, c_sz, ctypes.POINTER(Launch), c_vp]),
+    "fp_evaluate_batch_noalloc": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.POINTER(PlanSizes), c_vp, c_vp, c_vp,
+                                                 c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(Launch), c_vp]),
     "fp_read_status": (ctypes.c_int, [c_vp, ctypes.POINTER(c_i32), c_vp]),
     "fp_count_pairs": (ctypes.c_int, [c_vp, ctypes.POINTER(PlanSizes), c_vp, c_vp, c_vp, c_sz, c_vp, c_vp]),
     "fp_hmc_prepare": (ctypes.c_int, [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),

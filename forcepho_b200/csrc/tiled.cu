@@ -25,6 +25,8 @@
 //                  canonical order (FP64) -> chi2 (f64) and Response (f32).
 // No atomics touch the results, so they are bitwise reproducible.
 
+#include <atomic>
+
 #include "fp_common.cuh"
 #include "fp_gauss.cuh"
 
@@ -719,3 +721,53 @@ extern "C" int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches
     return FP_OK;
 }
 
+// ---------------------------------------------------------------------------
+// fp_evaluate_batch_noalloc: the same evaluation with a fixed scratch array
+// ---------------------------------------------------------------------------
+// Some callers cannot allocate device memory: a host-language binding that only
+// holds raw device pointers handed to it by another runtime (no CUDA allocator
+// on its side), or a process whose device memory is entirely reserved by
+// another allocator's pool, where an extra cudaMalloc fails or fragments it.
+// For them the workspace is this file-scope device array: every GPU that loads
+// the library holds it until the process exits.  All calls share it, and it
+// keeps the previous call's contents.
+static __device__ __align__(256) unsigned char g_noalloc_ws[FP_NOALLOC_WORKSPACE_BYTES];
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::atomic<void *> g_noalloc_addr[NOALLOC_MAX_DEVICES];
+}  // namespace
+
+extern "C" int fp_evaluate_batch_noalloc(const fp_patch *const *d_patches, int n_patches,
+                                         const fp_plan_sizes *sizes, const fp_exposure_desc *d_expos,
+                                         const fp_tile *d_tiles, const int32_t *d_order,
+                                         const fp_band_desc *d_bands, const fp_source *d_proposals,
+                                         double *d_chi2, fp_response *d_response, const fp_launch *launch,
+                                         void *stream)
+{
+    if (!sizes) return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch_noalloc: NULL sizes");
+    if (sizes->workspace_bytes < 0 || (uint64_t)sizes->workspace_bytes > (uint64_t)FP_NOALLOC_WORKSPACE_BYTES)
+        return fp_set_error(FP_ERR_WORKSPACE,
+                            "fp_evaluate_batch_noalloc: the plan needs %lld B of workspace, more than the fixed "
+                            "%llu B array; use fp_evaluate_batch with a caller-allocated workspace",
+                            (long long)sizes->workspace_bytes, (unsigned long long)FP_NOALLOC_WORKSPACE_BYTES);
+    int dev = 0;
+    if (int rc = fp_check_cuda(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch_noalloc: device %d beyond %d", dev,
+                            NOALLOC_MAX_DEVICES);
+    // set-up, once per device, with that device current: the array's device
+    // address (its name in host code is only a host-side stand-in)
+    void *ws = g_noalloc_addr[dev].load();
+    if (ws == nullptr) {
+        if (int rc = fp_check_cuda(cudaGetSymbolAddress(&ws, g_noalloc_ws), "cudaGetSymbolAddress(noalloc workspace)"))
+            return rc;
+        g_noalloc_addr[dev].store(ws);
+    }
+    // the control block (work-queue counter, status word) must start at zero
+    if (int rc = fp_check_cuda(cudaMemsetAsync(ws, 0, sizeof(fp_control), (cudaStream_t)stream),
+                               "fp_evaluate_batch_noalloc: clear control block"))
+        return rc;
+    return fp_evaluate_batch(d_patches, n_patches, sizes, d_expos, d_tiles, d_order, d_bands, d_proposals, d_chi2,
+                             d_response, ws, (size_t)FP_NOALLOC_WORKSPACE_BYTES, launch, stream);
+}

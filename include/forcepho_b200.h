@@ -362,6 +362,35 @@ typedef struct fp_hmc_state {
 FP_API int fp_hmc_leapfrog(const fp_hmc_patch *d_hp, int n_patches, const fp_hmc_state *state, int stage,
                            void *stream);
 
+/* Size of the fixed device scratch array of fp_evaluate_batch_noalloc (32 MiB). */
+#define FP_NOALLOC_WORKSPACE_BYTES (32u << 20)
+
+/* fp_evaluate_batch without a workspace argument, for callers that cannot
+ * allocate device memory: a host-language binding that only holds raw device
+ * pointers given to it by another runtime and has no CUDA allocator of its
+ * own, or a process whose device memory is all reserved by another
+ * allocator's pool, where an extra cudaMalloc would fail or fragment it.
+ * No counterpart in the reference (its kernel needs no scratch memory).
+ *
+ * The scratch is a file-scope device array of FP_NOALLOC_WORKSPACE_BYTES that
+ * every GPU loading the library holds until the process exits.  Plans whose
+ * sizes->workspace_bytes exceed it are rejected with FP_ERR_WORKSPACE (a
+ * single patch of 30 sources x 8 bands x 4 exposures of 256x256 pixels needs
+ * about 15 MB; a 512-patch batch does not fit).  The caller still passes all
+ * inputs and outputs; nothing is allocated or freed.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current, so make that first call before any stream capture.  All
+ * calls share the array and it keeps the previous call's contents (the call
+ * clears the part that must start at zero): calls that overlap on the GPU, on
+ * different streams or from different threads, race and corrupt each other's
+ * results. */
+FP_API int fp_evaluate_batch_noalloc(const fp_patch *const *d_patches, int n_patches,
+                                     const fp_plan_sizes *sizes, const fp_exposure_desc *d_expos,
+                                     const fp_tile *d_tiles, const int32_t *d_order,
+                                     const fp_band_desc *d_bands, const fp_source *d_proposals,
+                                     double *d_chi2, fp_response *d_response, const fp_launch *launch,
+                                     void *stream);
+
 /* Read and clear the device status word written by the batched kernels
  * (0 = no inconsistency seen).  Synchronises `stream`. */
 FP_API int fp_read_status(void *d_workspace, int32_t *status_out, void *stream);
