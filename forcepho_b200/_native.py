@@ -19,13 +19,17 @@ c_i32, c_i64, c_vp, c_sz = ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p, ctyp
 class PatchShape(ctypes.Structure):
     _fields_ = [("n_bands", c_i32), ("n_exposures", c_i32), ("n_sources", c_i32), ("n_pix", c_i32),
                 ("exposure_start", c_vp), ("exposure_N", c_vp), ("band_start", c_vp),
-                ("band_N", c_vp), ("n_psf_per_source", c_vp)]
+                ("band_N", c_vp), ("n_psf_per_source", c_vp), ("xpix", c_vp), ("ypix", c_vp)]
 
 
 class PlanSizes(ctypes.Structure):
     _fields_ = [("n_exposures", c_i64), ("n_tiles", c_i64), ("n_band_outputs", c_i64),
                 ("n_gauss", c_i64), ("n_pairs", c_i64), ("n_partials", c_i64),
-                ("max_gauss", c_i64), ("workspace_bytes", c_i64)]
+                ("max_gauss", c_i64), ("workspace_bytes", c_i64), ("n_perm", c_i64)]
+
+
+class PlanTables(ctypes.Structure):
+    _fields_ = [("expos", c_vp), ("tiles", c_vp), ("order", c_vp), ("bands", c_vp), ("perm", c_vp)]
 
 
 class Launch(ctypes.Structure):
@@ -59,7 +63,7 @@ FP_OK, FP_ERR_ARGUMENT, FP_ERR_LIMITS, FP_ERR_CUDA, FP_ERR_WORKSPACE, FP_ERR_DEV
 exposure_desc_dtype = np.dtype([("gauss_offset", np.int64), ("patch", np.int32), ("exposure", np.int32),
                                 ("band", np.int32), ("n_gauss", np.int32), ("n_psf", np.int32),
                                 ("n_sources", np.int32)])
-tile_dtype = np.dtype([("partial_offset", np.int64), ("expo", np.int32), ("pix_start", np.int32),
+tile_dtype = np.dtype([("partial_offset", np.int64), ("expo", np.int32), ("perm_start", np.int32),
                        ("n_pix", np.int32), ("pad", np.int32), ("bbox", np.float32, 4)])
 band_desc_dtype = np.dtype([("patch", np.int32), ("band", np.int32), ("tile_begin", np.int32),
                             ("tile_end", np.int32), ("n_sources", np.int32), ("pad", np.int32)])
@@ -72,15 +76,17 @@ SIGNATURES = {
     "fp_struct_sizes": (ctypes.c_int, [c_vp]),
     "fp_evaluate_proposal_plain": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp]),
     "fp_plan_count": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PlanSizes)]),
-    "fp_plan_fill": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp, c_vp]),
-    "fp_plan_bbox": (ctypes.c_int, [c_vp, c_vp, c_vp, c_i64, c_vp]),
+    "fp_plan_fill": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "fp_plan_bbox": (ctypes.c_int, [c_vp, ctypes.POINTER(PlanSizes), ctypes.POINTER(PlanTables), c_vp]),
     "fp_tile_smem_bytes": (ctypes.c_int, [ctypes.c_int, c_i64, ctypes.POINTER(c_i64)]),
-    "fp_evaluate_batch": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.POINTER(PlanSizes), c_vp, c_vp, c_vp,
-                                         c_vp, c_vp, c_vp, c_vp, c_vp, c_sz, ctypes.POINTER(Launch), c_vp]),
-    "fp_evaluate_batch_noalloc": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.POINTER(PlanSizes), c_vp, c_vp, c_vp,
-                                                 c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(Launch), c_vp]),
+    "fp_evaluate_batch": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.POINTER(PlanSizes), ctypes.POINTER(PlanTables),
+                                         c_vp, c_vp, c_vp, c_vp, c_sz, ctypes.POINTER(Launch), c_vp]),
+    "fp_evaluate_batch_noalloc": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.POINTER(PlanSizes),
+                                                 ctypes.POINTER(PlanTables), c_vp, c_vp, c_vp,
+                                                 ctypes.POINTER(Launch), c_vp]),
     "fp_read_status": (ctypes.c_int, [c_vp, ctypes.POINTER(c_i32), c_vp]),
-    "fp_count_pairs": (ctypes.c_int, [c_vp, ctypes.POINTER(PlanSizes), c_vp, c_vp, c_vp, c_sz, c_vp, c_vp]),
+    "fp_count_pairs": (ctypes.c_int, [c_vp, ctypes.POINTER(PlanSizes), ctypes.POINTER(PlanTables), c_vp, c_sz,
+                                      c_vp, c_vp]),
     "fp_hmc_prepare": (ctypes.c_int, [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "fp_hmc_lnprob": (ctypes.c_int, [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, ctypes.c_int, ctypes.c_int,
                                      c_vp, c_vp, c_vp]),
@@ -132,15 +138,19 @@ def check(rc, what=""):
     return rc
 
 
-def patch_shape(patch):
-    """PatchShape of a PatchBase; keeps the index arrays alive on the returned object."""
+def patch_shape(patch, coordinates=True):
+    """PatchShape of a PatchBase (with its pixel coordinates unless
+    ``coordinates`` is False); keeps the arrays alive on the returned object."""
     keep = [np.ascontiguousarray(patch.exposure_start, dtype=np.int32),
             np.ascontiguousarray(patch.exposure_N, dtype=np.int32),
             np.ascontiguousarray(patch.band_start, dtype=np.int16),
             np.ascontiguousarray(patch.band_N, dtype=np.int16),
-            np.ascontiguousarray(patch.n_psf_per_source, dtype=np.int32)]
+            np.ascontiguousarray(patch.n_psf_per_source, dtype=np.int32),
+            np.ascontiguousarray(patch.xpix, dtype=np.float32),
+            np.ascontiguousarray(patch.ypix, dtype=np.float32)]
+    xp, yp = (keep[5].ctypes.data, keep[6].ctypes.data) if coordinates else (None, None)
     s = PatchShape(patch.n_bands, patch.n_exp, int(patch.n_sources), patch.npix,
                    keep[0].ctypes.data, keep[1].ctypes.data, keep[2].ctypes.data, keep[3].ctypes.data,
-                   keep[4].ctypes.data)
+                   keep[4].ctypes.data, xp, yp)
     s._keep = keep
     return s

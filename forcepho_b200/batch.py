@@ -66,9 +66,8 @@ class BatchedProposer:
             pl.proposals.copy_(torch.from_numpy(props.view(np.uint8).reshape(-1)))
             return pl
 
-        probe = Plan(self.patches, tile_pixels=1024)
-        key = size_class(probe.n_pairs, probe.sizes.n_tiles)
-        del probe
+        n_pairs = sum(p.n_pairs() for p in self.patches)
+        key = size_class(n_pairs, sum(p.npix for p in self.patches) // 1024)
         tp, cps, ms = tuner.tune(key, make_plan)
         self.tune_log = [r for r in tuner.log if r[0] == key]
         self.plan = Plan(self.patches, tile_pixels=tp)
@@ -164,9 +163,9 @@ class BatchedProposer:
         self.plan.evaluate(self.launch, stream=s)
         counts = torch.zeros(3, dtype=torch.int64, device=self.plan.device)
         pl = self.plan
-        N.check(pl.L.fp_count_pairs(pl.d_patches.data_ptr(), ctypes.byref(pl.sizes), pl.d_expos.data_ptr(),
-                                    pl.d_tiles.data_ptr(), pl.workspace.data_ptr(), pl.workspace.numel(),
-                                    counts.data_ptr(), ctypes.c_void_p(s.cuda_stream)), "fp_count_pairs")
+        N.check(pl.L.fp_count_pairs(pl.d_patches.data_ptr(), ctypes.byref(pl.sizes), ctypes.byref(pl.tables),
+                                    pl.workspace.data_ptr(), pl.workspace.numel(), counts.data_ptr(),
+                                    ctypes.c_void_p(s.cuda_stream)), "fp_count_pairs")
         s.synchronize()
         return tuple(int(v) for v in counts.cpu())
 

@@ -86,7 +86,8 @@ setup_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc
 // tile bounding boxes (one-time, per plan)
 // ---------------------------------------------------------------------------
 __global__ void bbox_kernel(const fp_patch *const *__restrict__ patches,
-                            const fp_exposure_desc *__restrict__ expos, fp_tile *tiles, int64_t n_tiles)
+                            const fp_exposure_desc *__restrict__ expos, fp_tile *tiles,
+                            const int32_t *__restrict__ perm, int64_t n_tiles)
 {
     const int64_t t = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
     if (t >= n_tiles) return;
@@ -95,7 +96,8 @@ __global__ void bbox_kernel(const fp_patch *const *__restrict__ patches,
     const fp_patch *pt = patches[expos[tl.expo].patch];
     float x0 = INFINITY, x1 = -INFINITY, y0 = INFINITY, y1 = -INFINITY;
     for (int i = lane; i < tl.n_pix; i += 32) {
-        const float x = pt->xpix[tl.pix_start + i], y = pt->ypix[tl.pix_start + i];
+        const int32_t ix = perm[tl.perm_start + i];
+        const float x = pt->xpix[ix], y = pt->ypix[ix];
         x0 = fminf(x0, x); x1 = fmaxf(x1, x);
         y0 = fminf(y0, y); y1 = fmaxf(y1, y);
     }
@@ -114,43 +116,6 @@ __global__ void bbox_kernel(const fp_patch *const *__restrict__ patches,
 // ---------------------------------------------------------------------------
 // tile kernel helpers
 // ---------------------------------------------------------------------------
-template <int P>
-__device__ __forceinline__ void load_px(const float *__restrict__ src, bool vec, int nval, float (&v)[P])
-{
-    if (vec && nval >= P) {
-        if constexpr (P == 4) {
-            const float4 t = __ldg(reinterpret_cast<const float4 *>(src));
-            v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-        } else if constexpr (P == 2) {
-            const float2 t = __ldg(reinterpret_cast<const float2 *>(src));
-            v[0] = t.x; v[1] = t.y;
-        } else {
-            v[0] = __ldg(src);
-        }
-    } else {
-#pragma unroll
-        for (int k = 0; k < P; ++k) v[k] = (k < nval) ? __ldg(src + k) : 0.f;
-    }
-}
-
-template <int P>
-__device__ __forceinline__ void store_px(float *dst, bool vec, int nval, const float (&v)[P])
-{
-    if (vec && nval >= P) {
-        if constexpr (P == 4) {
-            *reinterpret_cast<float4 *>(dst) = make_float4(v[0], v[1], v[2], v[3]);
-        } else if constexpr (P == 2) {
-            *reinterpret_cast<float2 *>(dst) = make_float2(v[0], v[1]);
-        } else {
-            dst[0] = v[0];
-        }
-    } else {
-#pragma unroll
-        for (int k = 0; k < P; ++k)
-            if (k < nval) dst[k] = v[k];
-    }
-}
-
 // Adjoint moments of one Gaussian (params A, B) over pixels [p0, p1) of the
 // tile's nonzero-weight list.  With K = w' 2^(cE) (w' = -2 r ierr^2, zero past
 // the cutoff), H the pixel-integral factor and v' = c F dx:
@@ -221,7 +186,7 @@ __device__ __forceinline__ void moments_to_grad(const double *__restrict__ J, co
 }
 
 struct tile_smem {
-    size_t ga, gb, pix, slot, src, red, ints, idx, total;
+    size_t ga, gb, box, pix, slot, src, red, ints, idx, total;
 };
 
 __host__ __device__ inline tile_smem tile_smem_layout(int tile_pixels, int max_gauss)
@@ -230,6 +195,7 @@ __host__ __device__ inline tile_smem tile_smem_layout(int tile_pixels, int max_g
     size_t o = 0;
     L.ga = o;   o += (size_t)FP_CHUNK * 16;
     L.gb = o;   o += (size_t)FP_CHUNK * 16;
+    L.box = o;  o += (size_t)FP_CHUNK * 16;
     L.pix = o;  o += (size_t)tile_pixels * 16;
     L.slot = o; o += (size_t)SLOT_GROUPS * 32 * NPARAMS * 8;
     L.src = o;  o += (size_t)MAXSOURCES * NPARAMS * 8;
@@ -246,7 +212,8 @@ __host__ __device__ inline tile_smem tile_smem_layout(int tile_pixels, int max_g
 template <int P>
 __global__ void __launch_bounds__(FP_THREADS, 3)
 tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc *__restrict__ expos,
-            const fp_tile *__restrict__ tiles, const int32_t *__restrict__ order, int64_t n_tiles,
+            const fp_tile *__restrict__ tiles, const int32_t *__restrict__ order,
+            const int32_t *__restrict__ perm, int64_t n_tiles,
             const float4 *__restrict__ gfwd, const float4 *__restrict__ gbox,
             const double *__restrict__ gjac, double *__restrict__ partials, fp_control *ctl,
             int max_gauss, int flags)
@@ -256,6 +223,7 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
     const tile_smem L = tile_smem_layout(T, max_gauss);
     float4 *s_ga = reinterpret_cast<float4 *>(smem + L.ga);
     float4 *s_gb = reinterpret_cast<float4 *>(smem + L.gb);
+    float4 *s_gbox = reinterpret_cast<float4 *>(smem + L.box);
     float4 *s_pix = reinterpret_cast<float4 *>(smem + L.pix);
     double *s_slot = reinterpret_cast<double *>(smem + L.slot);
     double *s_src = reinterpret_cast<double *>(smem + L.src);
@@ -321,22 +289,38 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
         }
 
         // ---- 2. forward: model of P pixels per thread ----
+        // the tile's pixels are listed in the plan's pixel order (compact cells)
         const int j0 = tid * P;
         const int nval = npix - j0;
-        const int gp0 = tl.pix_start + j0;
-        const bool vec = ((((uintptr_t)(pt->xpix + tl.pix_start)) | ((uintptr_t)(pt->ypix + tl.pix_start)) |
-                           ((uintptr_t)(pt->data + tl.pix_start)) | ((uintptr_t)(pt->ierr + tl.pix_start))) &
-                          (4 * P - 1)) == 0;
+        const int32_t *tperm = perm + tl.perm_start + j0;
+        int idx[P];
         float xs[P], ys[P], ds[P], es[P];
-        if (nval > 0) {
-            load_px<P>(pt->xpix + gp0, vec, nval, xs);
-            load_px<P>(pt->ypix + gp0, vec, nval, ys);
-            load_px<P>(pt->data + gp0, vec, nval, ds);
-            load_px<P>(pt->ierr + gp0, vec, nval, es);
-        } else {
 #pragma unroll
-            for (int k = 0; k < P; ++k) xs[k] = ys[k] = ds[k] = es[k] = 0.f;
+        for (int k = 0; k < P; ++k) {
+            idx[k] = (k < nval) ? __ldg(tperm + k) : -1;
+            const bool ok = idx[k] >= 0;
+            xs[k] = ok ? __ldg(pt->xpix + idx[k]) : 0.f;
+            ys[k] = ok ? __ldg(pt->ypix + idx[k]) : 0.f;
+            ds[k] = ok ? __ldg(pt->data + idx[k]) : 0.f;
+            es[k] = ok ? __ldg(pt->ierr + idx[k]) : 0.f;
         }
+        // this warp's pixel box: Gaussians whose box misses it are skipped by
+        // the whole warp (they have E > MAX_EXP_ARG at all of its pixels)
+        float wx0 = INFINITY, wx1 = -INFINITY, wy0 = INFINITY, wy1 = -INFINITY;
+#pragma unroll
+        for (int k = 0; k < P; ++k)
+            if (k < nval) {
+                wx0 = fminf(wx0, xs[k]); wx1 = fmaxf(wx1, xs[k]);
+                wy0 = fminf(wy0, ys[k]); wy1 = fmaxf(wy1, ys[k]);
+            }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            wx0 = fminf(wx0, __shfl_xor_sync(0xffffffffu, wx0, o));
+            wx1 = fmaxf(wx1, __shfl_xor_sync(0xffffffffu, wx1, o));
+            wy0 = fminf(wy0, __shfl_xor_sync(0xffffffffu, wy0, o));
+            wy1 = fmaxf(wy1, __shfl_xor_sync(0xffffffffu, wy1, o));
+        }
+        if (nocull) { wx0 = wy0 = -INFINITY; wx1 = wy1 = INFINITY; }
         double M[P];
 #pragma unroll
         for (int k = 0; k < P; ++k) M[k] = 0.0;
@@ -348,6 +332,7 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
                 const int64_t gi = ed.gauss_offset + s_idx[c0 + i];
                 s_ga[i] = gfwd[2 * gi];
                 s_gb[i] = gfwd[2 * gi + 1];
+                s_gbox[i] = gbox[gi];
             }
             __syncthreads();
             if (nval > 0) {
@@ -356,8 +341,9 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
                     float m[P];
 #pragma unroll
                     for (int k = 0; k < P; ++k) m[k] = 0.f;
-#pragma unroll 2
                     for (int i = r0; i < r1; ++i) {
+                        const float4 bx = s_gbox[i];
+                        if (bx.y < wx0 || bx.x > wx1 || bx.w < wy0 || bx.z > wy1) continue;
                         const float4 A = s_ga[i], B = s_gb[i];
 #pragma unroll
                         for (int k = 0; k < P; ++k) {
@@ -392,9 +378,10 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
             ws[k] = live ? -2.f * ((r * es[k]) * es[k]) : 0.f;
             nz += (ws[k] != 0.f) ? 1 : 0;
         }
-        if (pt->residual != nullptr && nval > 0) {
-            const bool rvec = vec && ((((uintptr_t)(pt->residual + tl.pix_start)) & (4 * P - 1)) == 0);
-            store_px<P>(pt->residual + gp0, rvec, nval, rs);
+        if (pt->residual != nullptr) {
+#pragma unroll
+            for (int k = 0; k < P; ++k)
+                if (idx[k] >= 0) pt->residual[idx[k]] = rs[k];
         }
 
         // compact nonzero-weight pixels (ascending) into s_pix; reduce chi2 (fixed tree)
@@ -540,15 +527,16 @@ reduce_kernel(const fp_band_desc *__restrict__ bands, const fp_tile *__restrict_
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 count_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc *__restrict__ expos,
-             const fp_tile *__restrict__ tiles, const float4 *__restrict__ gfwd,
-             const float4 *__restrict__ gbox, unsigned long long *counts)
+             const fp_tile *__restrict__ tiles, const int32_t *__restrict__ perm,
+             const float4 *__restrict__ gfwd, const float4 *__restrict__ gbox, unsigned long long *counts)
 {
     const fp_tile tl = tiles[blockIdx.x];
     const fp_exposure_desc ed = expos[tl.expo];
     const fp_patch *pt = patches[ed.patch];
     unsigned long long inbox = 0, active = 0, bad = 0;
     for (int j = threadIdx.x; j < tl.n_pix; j += blockDim.x) {
-        const float x = pt->xpix[tl.pix_start + j], y = pt->ypix[tl.pix_start + j];
+        const int32_t ix = perm[tl.perm_start + j];
+        const float x = pt->xpix[ix], y = pt->ypix[ix];
         for (int g = 0; g < ed.n_gauss; ++g) {
             const int64_t gi = ed.gauss_offset + g;
             const float4 b = gbox[gi];
@@ -584,9 +572,8 @@ bool g_attr_set[8][3];
 
 template <int P>
 int launch_tiles(int grid, size_t smem, cudaStream_t st, const fp_patch *const *d_patches,
-                 const fp_exposure_desc *d_expos, const fp_tile *d_tiles, const int32_t *d_order,
-                 int64_t n_tiles, const float4 *gfwd, const float4 *gbox, const double *gjac,
-                 double *partials, fp_control *ctl, int max_gauss, int flags)
+                 const fp_plan_tables &tb, int64_t n_tiles, const float4 *gfwd, const float4 *gbox,
+                 const double *gjac, double *partials, fp_control *ctl, int max_gauss, int flags)
 {
     int dev = 0;
     if (int rc = fp_check_cuda(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
@@ -602,22 +589,30 @@ int launch_tiles(int grid, size_t smem, cudaStream_t st, const fp_patch *const *
             return rc;
         g_attr_set[dev][pi] = true;
     }
-    tile_kernel<P><<<grid, FP_THREADS, smem, st>>>(d_patches, d_expos, d_tiles, d_order, n_tiles, gfwd, gbox,
-                                                    gjac, partials, ctl, max_gauss, flags);
+    tile_kernel<P><<<grid, FP_THREADS, smem, st>>>(d_patches, tb.expos, tb.tiles, tb.order, tb.perm, n_tiles,
+                                                    gfwd, gbox, gjac, partials, ctl, max_gauss, flags);
     return fp_check_cuda(cudaGetLastError(), "tile_kernel launch");
 }
 
 }  // namespace
 
-extern "C" int fp_plan_bbox(const fp_patch *const *d_patches, const fp_exposure_desc *d_expos,
-                            fp_tile *d_tiles, int64_t n_tiles, void *stream)
+static int check_tables(const fp_plan_tables *tb, const char *who)
 {
-    if (!d_patches || !d_expos || !d_tiles || n_tiles < 0)
-        return fp_set_error(FP_ERR_ARGUMENT, "fp_plan_bbox: bad arguments");
-    if (n_tiles == 0) return FP_OK;
+    if (!tb || !tb->expos || !tb->tiles || !tb->order || !tb->bands || !tb->perm)
+        return fp_set_error(FP_ERR_ARGUMENT, "%s: NULL plan table", who);
+    return FP_OK;
+}
+
+extern "C" int fp_plan_bbox(const fp_patch *const *d_patches, const fp_plan_sizes *sizes,
+                            const fp_plan_tables *tables, void *stream)
+{
+    if (!d_patches || !sizes || sizes->n_tiles < 0) return fp_set_error(FP_ERR_ARGUMENT, "fp_plan_bbox: bad arguments");
+    if (int rc = check_tables(tables, "fp_plan_bbox")) return rc;
+    if (sizes->n_tiles == 0) return FP_OK;
     const int per_block = 8;
-    const int64_t grid = (n_tiles + per_block - 1) / per_block;
-    bbox_kernel<<<(unsigned)grid, 32 * per_block, 0, (cudaStream_t)stream>>>(d_patches, d_expos, d_tiles, n_tiles);
+    const int64_t grid = (sizes->n_tiles + per_block - 1) / per_block;
+    bbox_kernel<<<(unsigned)grid, 32 * per_block, 0, (cudaStream_t)stream>>>(d_patches, tables->expos, tables->tiles,
+                                                                          tables->perm, sizes->n_tiles);
     return fp_check_cuda(cudaGetLastError(), "bbox_kernel launch");
 }
 
@@ -629,32 +624,33 @@ extern "C" int fp_tile_smem_bytes(int tile_pixels, int64_t max_gauss, int64_t *o
 }
 
 extern "C" int fp_count_pairs(const fp_patch *const *d_patches, const fp_plan_sizes *sizes,
-                              const fp_exposure_desc *d_expos, const fp_tile *d_tiles, const void *d_workspace,
-                              size_t workspace_bytes, unsigned long long *d_counts, void *stream)
+                              const fp_plan_tables *tables, const void *d_workspace, size_t workspace_bytes,
+                              unsigned long long *d_counts, void *stream)
 {
-    if (!d_patches || !sizes || !d_expos || !d_tiles || !d_workspace || !d_counts)
+    if (!d_patches || !sizes || !d_workspace || !d_counts)
         return fp_set_error(FP_ERR_ARGUMENT, "fp_count_pairs: NULL argument");
+    if (int rc = check_tables(tables, "fp_count_pairs")) return rc;
     const fp_workspace_layout L = fp_layout(sizes->n_gauss, sizes->n_partials);
     if (workspace_bytes < L.total) return fp_set_error(FP_ERR_WORKSPACE, "fp_count_pairs: workspace too small");
     if (sizes->n_tiles <= 0) return FP_OK;
     if (sizes->n_tiles > INT32_MAX) return fp_set_error(FP_ERR_LIMITS, "fp_count_pairs: too many tiles");
     const unsigned char *ws = reinterpret_cast<const unsigned char *>(d_workspace);
     count_kernel<<<(unsigned)sizes->n_tiles, 256, 0, (cudaStream_t)stream>>>(
-        d_patches, d_expos, d_tiles, reinterpret_cast<const float4 *>(ws + L.gauss_fwd),
+        d_patches, tables->expos, tables->tiles, tables->perm, reinterpret_cast<const float4 *>(ws + L.gauss_fwd),
         reinterpret_cast<const float4 *>(ws + L.gauss_box), d_counts);
     return fp_check_cuda(cudaGetLastError(), "count_kernel launch");
 }
 
 extern "C" int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches, const fp_plan_sizes *sizes,
-                                 const fp_exposure_desc *d_expos, const fp_tile *d_tiles,
-                                 const int32_t *d_order, const fp_band_desc *d_bands,
-                                 const fp_source *d_proposals, double *d_chi2, fp_response *d_response,
-                                 void *d_workspace, size_t workspace_bytes, const fp_launch *launch,
-                                 void *stream)
+                                 const fp_plan_tables *tables, const fp_source *d_proposals, double *d_chi2,
+                                 fp_response *d_response, void *d_workspace, size_t workspace_bytes,
+                                 const fp_launch *launch, void *stream)
 {
-    if (!d_patches || n_patches < 1 || !sizes || !d_expos || !d_tiles || !d_order || !d_bands ||
-        !d_proposals || !d_chi2 || !d_response || !d_workspace || !launch)
+    if (!d_patches || n_patches < 1 || !sizes || !d_proposals || !d_chi2 || !d_response || !d_workspace ||
+        !launch)
         return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch: NULL argument");
+    if (int rc = check_tables(tables, "fp_evaluate_batch")) return rc;
+    const fp_plan_tables &tb = *tables;
     if (((uintptr_t)d_workspace) & 255)
         return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch: workspace must be 256-byte aligned");
     const fp_workspace_layout L = fp_layout(sizes->n_gauss, sizes->n_partials);
@@ -689,7 +685,7 @@ extern "C" int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches
     const int phases = launch->phases ? launch->phases : (FP_PHASE_SETUP | FP_PHASE_TILES | FP_PHASE_REDUCE);
     if ((phases & FP_PHASE_SETUP) && sizes->n_exposures > 0) {
         if (sizes->n_exposures > INT32_MAX) return fp_set_error(FP_ERR_LIMITS, "too many exposures");
-        setup_kernel<<<(unsigned)sizes->n_exposures, 256, 0, st>>>(d_patches, d_expos, d_proposals, gfwd, gbox,
+        setup_kernel<<<(unsigned)sizes->n_exposures, 256, 0, st>>>(d_patches, tb.expos, d_proposals, gfwd, gbox,
                                                                    gjac, ctl);
         if (int rc = fp_check_cuda(cudaGetLastError(), "setup_kernel launch")) return rc;
     }
@@ -703,18 +699,18 @@ extern "C" int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches
         int rc;
         const int mg = (int)sizes->max_gauss;
         if (T == 256)
-            rc = launch_tiles<1>(grid, smem, st, d_patches, d_expos, d_tiles, d_order, sizes->n_tiles, gfwd, gbox,
-                                 gjac, partials, ctl, mg, launch->flags);
+            rc = launch_tiles<1>(grid, smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gjac, partials, ctl,
+                                 mg, launch->flags);
         else if (T == 512)
-            rc = launch_tiles<2>(grid, smem, st, d_patches, d_expos, d_tiles, d_order, sizes->n_tiles, gfwd, gbox,
-                                 gjac, partials, ctl, mg, launch->flags);
+            rc = launch_tiles<2>(grid, smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gjac, partials, ctl,
+                                 mg, launch->flags);
         else
-            rc = launch_tiles<4>(grid, smem, st, d_patches, d_expos, d_tiles, d_order, sizes->n_tiles, gfwd, gbox,
-                                 gjac, partials, ctl, mg, launch->flags);
+            rc = launch_tiles<4>(grid, smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gjac, partials, ctl,
+                                 mg, launch->flags);
         if (rc) return rc;
     }
     if ((phases & FP_PHASE_REDUCE) && sizes->n_band_outputs > 0) {
-        reduce_kernel<<<(unsigned)sizes->n_band_outputs, REDUCE_THREADS, 0, st>>>(d_bands, d_tiles, partials,
+        reduce_kernel<<<(unsigned)sizes->n_band_outputs, REDUCE_THREADS, 0, st>>>(tb.bands, tb.tiles, partials,
                                                                                   d_chi2, d_response);
         if (int rc = fp_check_cuda(cudaGetLastError(), "reduce_kernel launch")) return rc;
     }
@@ -739,11 +735,9 @@ std::atomic<void *> g_noalloc_addr[NOALLOC_MAX_DEVICES];
 }  // namespace
 
 extern "C" int fp_evaluate_batch_noalloc(const fp_patch *const *d_patches, int n_patches,
-                                         const fp_plan_sizes *sizes, const fp_exposure_desc *d_expos,
-                                         const fp_tile *d_tiles, const int32_t *d_order,
-                                         const fp_band_desc *d_bands, const fp_source *d_proposals,
-                                         double *d_chi2, fp_response *d_response, const fp_launch *launch,
-                                         void *stream)
+                                         const fp_plan_sizes *sizes, const fp_plan_tables *tables,
+                                         const fp_source *d_proposals, double *d_chi2, fp_response *d_response,
+                                         const fp_launch *launch, void *stream)
 {
     if (!sizes) return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch_noalloc: NULL sizes");
     if (sizes->workspace_bytes < 0 || (uint64_t)sizes->workspace_bytes > (uint64_t)FP_NOALLOC_WORKSPACE_BYTES)
@@ -768,6 +762,6 @@ extern "C" int fp_evaluate_batch_noalloc(const fp_patch *const *d_patches, int n
     if (int rc = fp_check_cuda(cudaMemsetAsync(ws, 0, sizeof(fp_control), (cudaStream_t)stream),
                                "fp_evaluate_batch_noalloc: clear control block"))
         return rc;
-    return fp_evaluate_batch(d_patches, n_patches, sizes, d_expos, d_tiles, d_order, d_bands, d_proposals, d_chi2,
-                             d_response, ws, (size_t)FP_NOALLOC_WORKSPACE_BYTES, launch, stream);
+    return fp_evaluate_batch(d_patches, n_patches, sizes, tables, d_proposals, d_chi2, d_response, ws,
+                             (size_t)FP_NOALLOC_WORKSPACE_BYTES, launch, stream);
 }

@@ -169,14 +169,14 @@ class Plan:
     the output buffers ``chi2`` f64[n_patches, MAXBANDS] and ``response``
     f32[n_patches, MAXBANDS, MAXSOURCES*NPARAMS]."""
 
-    def __init__(self, patches, tile_pixels=1024, device=None, stream=None):
+    def __init__(self, patches, tile_pixels=1024, device=None, stream=None, compact_tiles=True):
         self.L = N.load()
         self.patches = list(patches)
         self.n = len(self.patches)
         self.tile_pixels = int(tile_pixels)
         dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.device = dev
-        shapes = [N.patch_shape(p) for p in self.patches]
+        shapes = [N.patch_shape(p, coordinates=compact_tiles) for p in self.patches]
         self._shapes = (N.PatchShape * self.n)(*shapes)
         self._shape_keep = shapes
         sz = N.PlanSizes()
@@ -187,19 +187,24 @@ class Plan:
         h_tiles = np.zeros(sz.n_tiles, dtype=N.tile_dtype)
         h_bands = np.zeros(sz.n_band_outputs, dtype=N.band_desc_dtype)
         h_order = np.zeros(sz.n_tiles, dtype=np.int32)
+        h_perm = np.zeros(sz.n_perm, dtype=np.int32)
         N.check(self.L.fp_plan_fill(ctypes.addressof(self._shapes), self.n, self.tile_pixels,
                                     h_expos.ctypes.data, h_tiles.ctypes.data, h_bands.ctypes.data,
-                                    h_order.ctypes.data), "fp_plan_fill")
+                                    h_order.ctypes.data, h_perm.ctypes.data), "fp_plan_fill")
         self.h_expos, self.h_tiles, self.h_bands, self.h_order = h_expos, h_tiles, h_bands, h_order
+        self.h_perm = h_perm
         self.d_expos = to_device_bytes(h_expos, dev)
         self.d_tiles = to_device_bytes(h_tiles, dev)
         self.d_bands = to_device_bytes(h_bands, dev)
         self.d_order = to_device_bytes(h_order, dev)
+        self.d_perm = to_device_bytes(h_perm, dev)
+        self.tables = N.PlanTables(_ptr(self.d_expos), _ptr(self.d_tiles), _ptr(self.d_order),
+                                   _ptr(self.d_bands), _ptr(self.d_perm))
         self.d_patches = torch.zeros(self.n, dtype=torch.int64, device=dev)
         self.refresh_patch_pointers()
         st = current_stream_ptr(stream)
-        N.check(self.L.fp_plan_bbox(_ptr(self.d_patches), _ptr(self.d_expos), _ptr(self.d_tiles),
-                                    sz.n_tiles, st), "fp_plan_bbox")
+        N.check(self.L.fp_plan_bbox(_ptr(self.d_patches), ctypes.byref(sz), ctypes.byref(self.tables), st),
+                "fp_plan_bbox")
         self.workspace = torch.zeros(max(sz.workspace_bytes, 256), dtype=torch.uint8, device=dev)
         self.proposals = torch.zeros(self.n * MAXSOURCES * source_struct_dtype.itemsize, dtype=torch.uint8,
                                      device=dev)
@@ -235,10 +240,9 @@ class Plan:
         c2 = self.chi2 if chi2 is None else chi2
         rs = self.response if response is None else response
         N.check(self.L.fp_evaluate_batch(
-            _ptr(self.d_patches), self.n, ctypes.byref(self.sizes), _ptr(self.d_expos), _ptr(self.d_tiles),
-            _ptr(self.d_order), _ptr(self.d_bands), _ptr(props), _ptr(c2), _ptr(rs),
-            _ptr(self.workspace), self.workspace.numel(), ctypes.byref(lp), current_stream_ptr(stream)),
-            "fp_evaluate_batch")
+            _ptr(self.d_patches), self.n, ctypes.byref(self.sizes), ctypes.byref(self.tables), _ptr(props),
+            _ptr(c2), _ptr(rs), _ptr(self.workspace), self.workspace.numel(), ctypes.byref(lp),
+            current_stream_ptr(stream)), "fp_evaluate_batch")
 
     def read_status(self, stream=None):
         st = ctypes.c_int32(0)

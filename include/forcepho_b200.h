@@ -157,10 +157,12 @@ FP_API int fp_evaluate_proposal_plain(const fp_patch *d_patch, const fp_source *
 /* Tiled / batched path.                                                     */
 /* ------------------------------------------------------------------------- */
 /* A "plan" covers one or many patches whose pixel layout is fixed.  It splits
- * every exposure into pixel tiles (the work items of one persistent launch) and
+ * every exposure into spatially compact pixel tiles (the work items of one
+ * persistent launch: square cells of the image plane, see fp_plan_count) and
  * lays out the workspace.  Planning runs on the host from the host copies of
- * each patch's index arrays; the caller copies the three host tables the plan
- * fills to device memory and passes them to fp_evaluate_batch. */
+ * each patch's index arrays and pixel coordinates; the caller copies the host
+ * tables the plan fills to device memory and passes them, as fp_plan_tables,
+ * to fp_evaluate_batch. */
 
 /* Host-side shape of one patch (pointers are host copies of the index arrays). */
 typedef struct fp_patch_shape {
@@ -173,6 +175,8 @@ typedef struct fp_patch_shape {
     const int16_t *band_start;          /* [n_bands] */
     const int16_t *band_N;              /* [n_bands] */
     const int32_t *n_psf_per_source;    /* [n_bands] */
+    const float *xpix;                  /* [n_pix] or NULL (then tiles are runs of consecutive pixels) */
+    const float *ypix;                  /* [n_pix] or NULL */
 } fp_patch_shape;
 
 /* Device descriptor of one exposure of one patch (planner output). */
@@ -186,11 +190,11 @@ typedef struct fp_exposure_desc {
     int32_t n_sources;
 } fp_exposure_desc;        /* 32 bytes */
 
-/* Device work item: one tile of consecutive pixels of one exposure. */
+/* Device work item: one tile of pixels of one exposure. */
 typedef struct fp_tile {
     int64_t partial_offset; /* first double of this tile's partials in the workspace */
     int32_t expo;           /* index into the plan's fp_exposure_desc table */
-    int32_t pix_start;      /* first pixel (index into the patch's pixel arrays) */
+    int32_t perm_start;     /* first entry of this tile in the plan's pixel order */
     int32_t n_pix;          /* pixels in the tile (<= tile_pixels) */
     int32_t pad;
     float bbox[4];          /* xmin, xmax, ymin, ymax of the tile's pixels (device-filled) */
@@ -216,25 +220,40 @@ typedef struct fp_plan_sizes {
     int64_t n_partials;     /* doubles of per-tile partial sums */
     int64_t max_gauss;      /* largest image-Gaussian count of one exposure */
     int64_t workspace_bytes;/* device workspace fp_evaluate_batch needs */
+    int64_t n_perm;         /* entries of the plan's pixel order (sum of exposure_N) */
 } fp_plan_sizes;
 
-/* Count the plan of `n_patches` patches split into tiles of `tile_pixels`
- * pixels (a multiple of 32, at most 4096). */
+/* The device copies of a plan's tables (a host struct of device pointers). */
+typedef struct fp_plan_tables {
+    const fp_exposure_desc *expos;  /* [n_exposures] */
+    fp_tile *tiles;                 /* [n_tiles], canonical order (patch, band, exposure, cell) */
+    const int32_t *order;           /* [n_tiles] execution order, most work first */
+    const fp_band_desc *bands;      /* [n_band_outputs] */
+    const int32_t *perm;            /* [n_perm] index within its patch of every tile pixel, tile after tile */
+} fp_plan_tables;
+
+/* Count the plan of `n_patches` patches split into tiles of at most
+ * `tile_pixels` pixels (a multiple of 32, at most 4096).  With pixel
+ * coordinates, each exposure's pixels are grouped into cells of the image
+ * plane (32x32 pixels for 1024-pixel tiles, 32x16 for 512, 16x16 for 256),
+ * cells taken row by row and pixels within a cell in their input order; a cell
+ * with more pixels than a tile is split. */
 FP_API int fp_plan_count(const fp_patch_shape *h_shapes, int n_patches, int tile_pixels,
                   fp_plan_sizes *out);
 
 /* Fill the host tables of a plan (sizes from fp_plan_count).  Tiles are emitted
- * in canonical order (patch, band, exposure, pixel); h_order receives an
- * execution order (largest estimated work first) of length n_tiles. */
+ * in canonical order (patch, band, exposure, cell); h_order receives an
+ * execution order (largest estimated work first) of length n_tiles, h_perm the
+ * plan's pixel order (n_perm entries). */
 FP_API int fp_plan_fill(const fp_patch_shape *h_shapes, int n_patches, int tile_pixels,
                  fp_exposure_desc *h_expos, fp_tile *h_tiles, fp_band_desc *h_bands,
-                 int32_t *h_order);
+                 int32_t *h_order, int32_t *h_perm);
 
 /* One-time device pass after the tables are uploaded: computes each tile's
- * pixel bounding box from the patch's xpix/ypix.  d_patches: device array of
- * n_patches device fp_patch pointers. */
-FP_API int fp_plan_bbox(const fp_patch *const *d_patches, const fp_exposure_desc *d_expos,
-                 fp_tile *d_tiles, int64_t n_tiles, void *stream);
+ * pixel bounding box (into tables->tiles) from the patch's xpix/ypix.
+ * d_patches: device array of n_patches device fp_patch pointers. */
+FP_API int fp_plan_bbox(const fp_patch *const *d_patches, const fp_plan_sizes *sizes,
+                        const fp_plan_tables *tables, void *stream);
 
 /* Launch parameters of the batched evaluation (chosen by the autotuner). */
 typedef struct fp_launch {
@@ -259,8 +278,7 @@ FP_API int fp_tile_smem_bytes(int tile_pixels, int64_t max_gauss, int64_t *out);
  * (Gaussian setup, one persistent tile launch, fixed-order reduction).
  *   d_patches     device array [n_patches] of device fp_patch pointers
  *   sizes         the plan's sizes (host struct from fp_plan_count)
- *   d_expos, d_tiles, d_order, d_bands   the plan's tables (device copies;
- *                 d_tiles after fp_plan_bbox)
+ *   tables        the plan's device tables (tiles after fp_plan_bbox)
  *   d_proposals   device fp_source[n_patches][MAXSOURCES] (rows >= n_sources unused)
  *   d_chi2        device f64[n_patches][MAXBANDS]        (bands >= n_bands untouched)
  *   d_response    device fp_response[n_patches][MAXBANDS]
@@ -269,8 +287,7 @@ FP_API int fp_tile_smem_bytes(int tile_pixels, int64_t max_gauss, int64_t *out);
  * launch (forcepho/proposal.py:96-152).  Results are bitwise reproducible for
  * fixed inputs and launch parameters. */
 FP_API int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches, const fp_plan_sizes *sizes,
-                      const fp_exposure_desc *d_expos, const fp_tile *d_tiles,
-                      const int32_t *d_order, const fp_band_desc *d_bands,
+                      const fp_plan_tables *tables,
                       const fp_source *d_proposals, double *d_chi2, fp_response *d_response,
                       void *d_workspace, size_t workspace_bytes, const fp_launch *launch,
                       void *stream);
@@ -281,7 +298,7 @@ FP_API int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches, co
  * [1] pairs within the MAX_EXP_ARG cutoff, [2] within-cutoff pairs of Gaussians
  * the cull dropped (0 unless culling is wrong).  No reference counterpart. */
 FP_API int fp_count_pairs(const fp_patch *const *d_patches, const fp_plan_sizes *sizes,
-                          const fp_exposure_desc *d_expos, const fp_tile *d_tiles,
+                          const fp_plan_tables *tables,
                           const void *d_workspace, size_t workspace_bytes,
                           unsigned long long *d_counts, void *stream);
 
@@ -385,9 +402,8 @@ FP_API int fp_hmc_leapfrog(const fp_hmc_patch *d_hp, int n_patches, const fp_hmc
  * different streams or from different threads, race and corrupt each other's
  * results. */
 FP_API int fp_evaluate_batch_noalloc(const fp_patch *const *d_patches, int n_patches,
-                                     const fp_plan_sizes *sizes, const fp_exposure_desc *d_expos,
-                                     const fp_tile *d_tiles, const int32_t *d_order,
-                                     const fp_band_desc *d_bands, const fp_source *d_proposals,
+                                     const fp_plan_sizes *sizes, const fp_plan_tables *tables,
+                                     const fp_source *d_proposals,
                                      double *d_chi2, fp_response *d_response, const fp_launch *launch,
                                      void *stream);
 

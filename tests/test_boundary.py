@@ -52,9 +52,9 @@ def test_struct_sizes_reported_by_library():
     assert list(out) == [152, 264, 840, 28]
 
 
-def plan(patches, tile):
+def plan(patches, tile, coordinates=True):
     L = N.load()
-    shapes = [N.patch_shape(p) for p in patches]
+    shapes = [N.patch_shape(p, coordinates=coordinates) for p in patches]
     arr = (N.PatchShape * len(shapes))(*shapes)
     sz = N.PlanSizes()
     rc = L.fp_plan_count(ctypes.addressof(arr), len(shapes), tile, ctypes.byref(sz))
@@ -64,47 +64,75 @@ def plan(patches, tile):
     ti = np.zeros(sz.n_tiles, N.tile_dtype)
     bd = np.zeros(sz.n_band_outputs, N.band_desc_dtype)
     od = np.zeros(sz.n_tiles, np.int32)
+    pm = np.zeros(sz.n_perm, np.int32)
     N.check(L.fp_plan_fill(ctypes.addressof(arr), len(shapes), tile, ex.ctypes.data, ti.ctypes.data,
-                           bd.ctypes.data, od.ctypes.data), "fill")
-    return 0, (sz, ex, ti, bd, od)
+                           bd.ctypes.data, od.ctypes.data, pm.ctypes.data), "fill")
+    return 0, (sz, ex, ti, bd, od, pm)
+
+
+CELL = {1024: (32, 32), 512: (32, 16), 256: (16, 16)}
 
 
 @pytest.mark.parametrize("tile", [256, 512, 1024])
-def test_planner_tables(tile):
+@pytest.mark.parametrize("coordinates", [True, False])
+def test_planner_tables(tile, coordinates):
     patches = S.config_batched(seed=7, n_patches=6)
-    rc, (sz, ex, ti, bd, od) = plan(patches, tile)
+    rc, (sz, ex, ti, bd, od, pm) = plan(patches, tile, coordinates)
     assert rc == 0
     assert sz.n_pairs == sum(p.n_pairs() for p in patches)
     assert sz.n_exposures == sum(p.n_exp for p in patches)
     assert sz.n_band_outputs == sum(p.n_bands for p in patches)
-    # every pixel of every exposure is covered exactly once, in canonical order
+    assert sz.n_perm == sum(p.npix for p in patches)
     k = 0
     for pi, p in enumerate(patches):
         ns = int(p.n_sources)
         for b in range(p.n_bands):
             e0, ne = int(p.band_start[b]), int(p.band_N[b])
             row = bd[[i for i in range(len(bd)) if bd["patch"][i] == pi and bd["band"][i] == b][0]]
-            assert row["tile_begin"] == k
+            assert row["tile_begin"] == k and row["n_sources"] == ns
             for e in range(e0, e0 + ne):
-                covered = 0
-                while covered < p.exposure_N[e]:
+                s0, n = int(p.exposure_start[e]), int(p.exposure_N[e])
+                seen = []
+                while len(seen) < n:
                     t = ti[k]
                     assert ex[t["expo"]]["patch"] == pi and ex[t["expo"]]["exposure"] == e
-                    assert t["pix_start"] == p.exposure_start[e] + covered
                     assert 0 < t["n_pix"] <= tile
-                    covered += t["n_pix"]
+                    pix = pm[t["perm_start"]:t["perm_start"] + t["n_pix"]]
+                    assert np.all((pix >= s0) & (pix < s0 + n))
+                    if coordinates:
+                        x, y = p.xpix[pix], p.ypix[pix]
+                        if np.all(x >= 0):      # a real cell (the pad pixels share their own)
+                            cw, ch = CELL[tile]
+                            assert x.max() - x.min() < cw and y.max() - y.min() < ch
+                    else:
+                        assert np.array_equal(pix, np.arange(s0 + len(seen), s0 + len(seen) + len(pix)))
+                    seen.extend(pix.tolist())
                     k += 1
+                # every pixel of the exposure exactly once
+                assert sorted(seen) == list(range(s0, s0 + n))
             assert row["tile_end"] == k
-            assert row["n_sources"] == ns
     assert k == sz.n_tiles
-    # partial offsets are dense with the per-patch stride
     stride = np.array([1 + 7 * ex[t["expo"]]["n_sources"] for t in ti])
     assert np.array_equal(ti["partial_offset"], np.concatenate([[0], np.cumsum(stride)[:-1]]))
     assert sz.n_partials == stride.sum()
-    # execution order: a permutation, largest work first
     assert sorted(od.tolist()) == list(range(sz.n_tiles))
     work = ti["n_pix"][od].astype(np.int64) * ex[ti["expo"][od]]["n_gauss"]
     assert np.all(np.diff(work) <= 0)
+
+
+def test_planner_sparse_and_nonfinite_coordinates():
+    """Far-apart pixels (sparse grid, sorted path) and non-finite coordinates
+    still yield every pixel exactly once."""
+    p = S.config_small(seed=1)
+    p.xpix = p.xpix.copy()
+    p.ypix = p.ypix.copy()
+    p.xpix[::97] *= 1e6
+    p.xpix[5] = np.nan
+    p.ypix[7] = np.inf
+    rc, (sz, ex, ti, bd, od, pm) = plan([p], 256)
+    assert rc == 0
+    assert sorted(pm.tolist()) == list(range(p.npix))
+    assert ti["n_pix"].sum() == p.npix
 
 
 def test_planner_rejects_bad_shapes():

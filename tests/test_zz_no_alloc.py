@@ -50,8 +50,7 @@ def test_noalloc_matches_workspace_entry_point():
         chi2 = torch.full_like(plan.chi2, np.nan)
         resp = torch.full_like(plan.response, np.nan)
         rc = L.fp_evaluate_batch_noalloc(plan.d_patches.data_ptr(), 1, ctypes.byref(plan.sizes),
-                                         plan.d_expos.data_ptr(), plan.d_tiles.data_ptr(), plan.d_order.data_ptr(),
-                                         plan.d_bands.data_ptr(), plan.proposals.data_ptr(), chi2.data_ptr(),
+                                         ctypes.byref(plan.tables), plan.proposals.data_ptr(), chi2.data_ptr(),
                                          resp.data_ptr(), ctypes.byref(launch), ctypes.c_void_p(stream.cuda_stream))
         assert rc == 0, L.fp_error_string().decode()
         torch.cuda.synchronize()
@@ -67,9 +66,8 @@ def test_noalloc_matches_workspace_entry_point():
 def test_noalloc_rejects_plans_beyond_the_array():
     from forcepho_b200 import _native as N
     L = N.load()
-    sz = N.PlanSizes(1, 1, 1, 1, 1, 1, 1, N.NOALLOC_WORKSPACE_BYTES + 256)
+    sz = N.PlanSizes(1, 1, 1, 1, 1, 1, 1, N.NOALLOC_WORKSPACE_BYTES + 256, 1)
     lp = N.Launch(1024, 3, 0, 0)
-    rc = L.fp_evaluate_batch_noalloc(None, 1, ctypes.byref(sz), None, None, None, None, None, None, None,
-                                     ctypes.byref(lp), None)
+    rc = L.fp_evaluate_batch_noalloc(None, 1, ctypes.byref(sz), None, None, None, None, ctypes.byref(lp), None)
     assert rc == N.FP_ERR_WORKSPACE
     assert "fixed" in L.fp_error_string().decode()
