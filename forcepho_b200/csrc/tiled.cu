@@ -185,6 +185,31 @@ __device__ __forceinline__ void moments_to_grad(const double *__restrict__ J, co
     g[6] = J[18] * SA;
 }
 
+// Whether the region {E = dx^T F dx <= MAX_EXP_ARG (1% margin)} of a Gaussian
+// (FP32 pixel-loop parameters A = (xc, yc, c Fxx, c Fxy), fys = c Fyy) meets
+// the rectangle [x0,x1] x [y0,y1]: the minimum of the convex quadratic over the
+// rectangle is at the centre if it lies inside, else on an edge, where it is a
+// clamped 1-D minimum.  FP64; non-finite results keep the Gaussian.
+__device__ __forceinline__ bool ellipse_meets_rect(const float4 A, float fys, float x0, float x1, float y0,
+                                                   float y1)
+{
+    const double ic = 1.0 / FP_EXP2_SCALE;
+    const double cx = A.x, cy = A.y, fxx = A.z * ic, fxy = A.w * ic, fyy = fys * ic;
+    if (cx >= x0 && cx <= x1 && cy >= y0 && cy <= y1) return true;
+    double best = INFINITY;
+    const double lx = x0 - cx, hx = x1 - cx, ly = y0 - cy, hy = y1 - cy;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const double dx = k ? hx : lx;
+        const double dy = fmin(fmax(-fxy * dx / fyy, ly), hy);
+        best = fmin(best, fxx * dx * dx + 2.0 * fxy * dx * dy + fyy * dy * dy);
+        const double ey = k ? hy : ly;
+        const double ex = fmin(fmax(-fxy * ey / fxx, lx), hx);
+        best = fmin(best, fxx * ex * ex + 2.0 * fxy * ex * ey + fyy * ey * ey);
+    }
+    return !(best > MAX_EXP_ARG * 1.01);
+}
+
 struct tile_smem {
     size_t ga, gb, box, pix, slot, src, red, ints, idx, total;
 };
@@ -271,6 +296,9 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
                 } else {
                     const float4 b = gbox[ed.gauss_offset + g];
                     keep = (b.y >= bx0) && (b.x <= bx1) && (b.w >= by0) && (b.z <= by1);
+                    if (keep && isfinite(b.x))
+                        keep = ellipse_meets_rect(gfwd[2 * (ed.gauss_offset + g)],
+                                                  gfwd[2 * (ed.gauss_offset + g) + 1].x, bx0, bx1, by0, by1);
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, keep);
@@ -530,17 +558,26 @@ count_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc
              const fp_tile *__restrict__ tiles, const int32_t *__restrict__ perm,
              const float4 *__restrict__ gfwd, const float4 *__restrict__ gbox, unsigned long long *counts)
 {
+    extern __shared__ unsigned char s_keep[];   // [n_gauss]: the tile kernel's cull decision
     const fp_tile tl = tiles[blockIdx.x];
     const fp_exposure_desc ed = expos[tl.expo];
     const fp_patch *pt = patches[ed.patch];
+    const float bx0 = tl.bbox[0], bx1 = tl.bbox[1], by0 = tl.bbox[2], by1 = tl.bbox[3];
+    for (int g = threadIdx.x; g < ed.n_gauss; g += blockDim.x) {
+        const int64_t gi = ed.gauss_offset + g;
+        const float4 b = gbox[gi];
+        bool keep = (b.y >= bx0) && (b.x <= bx1) && (b.w >= by0) && (b.z <= by1);
+        if (keep && isfinite(b.x)) keep = ellipse_meets_rect(gfwd[2 * gi], gfwd[2 * gi + 1].x, bx0, bx1, by0, by1);
+        s_keep[g] = keep ? 1 : 0;
+    }
+    __syncthreads();
     unsigned long long inbox = 0, active = 0, bad = 0;
     for (int j = threadIdx.x; j < tl.n_pix; j += blockDim.x) {
         const int32_t ix = perm[tl.perm_start + j];
         const float x = pt->xpix[ix], y = pt->ypix[ix];
         for (int g = 0; g < ed.n_gauss; ++g) {
             const int64_t gi = ed.gauss_offset + g;
-            const float4 b = gbox[gi];
-            const bool keep = (b.y >= tl.bbox[0]) && (b.x <= tl.bbox[1]) && (b.w >= tl.bbox[2]) && (b.z <= tl.bbox[3]);
+            const bool keep = s_keep[g] != 0;
             const float4 A = gfwd[2 * gi], B = gfwd[2 * gi + 1];
             const float dx = x - A.x, dy = y - A.y;
             const float vx = fmaf(A.z, dx, A.w * dy);
@@ -635,7 +672,13 @@ extern "C" int fp_count_pairs(const fp_patch *const *d_patches, const fp_plan_si
     if (sizes->n_tiles <= 0) return FP_OK;
     if (sizes->n_tiles > INT32_MAX) return fp_set_error(FP_ERR_LIMITS, "fp_count_pairs: too many tiles");
     const unsigned char *ws = reinterpret_cast<const unsigned char *>(d_workspace);
-    count_kernel<<<(unsigned)sizes->n_tiles, 256, 0, (cudaStream_t)stream>>>(
+    const size_t keep_bytes = (size_t)(sizes->max_gauss > 0 ? sizes->max_gauss : 1);
+    if (keep_bytes > 48 * 1024)
+        if (int rc = fp_check_cuda(cudaFuncSetAttribute(count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        (int)keep_bytes),
+                                   "cudaFuncSetAttribute(count_kernel)"))
+            return rc;
+    count_kernel<<<(unsigned)sizes->n_tiles, 256, keep_bytes, (cudaStream_t)stream>>>(
         d_patches, tables->expos, tables->tiles, tables->perm, reinterpret_cast<const float4 *>(ws + L.gauss_fwd),
         reinterpret_cast<const float4 *>(ws + L.gauss_box), d_counts);
     return fp_check_cuda(cudaGetLastError(), "count_kernel launch");
