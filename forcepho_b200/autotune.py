@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 TILE_CHOICES = (256, 512, 1024)
-CTA_CHOICES = (2, 3)
+CTA_CHOICES = (3, 4)
 
 
 def size_class(n_pairs, n_tiles_at_1024):

@@ -38,7 +38,7 @@ class BatchedProposer:
     use_graph : capture the evaluation into a CUDA graph on first use.
     """
 
-    def __init__(self, patches, tile_pixels=1024, ctas_per_sm=3, flags=0, autotune=False,
+    def __init__(self, patches, tile_pixels=1024, ctas_per_sm=4, flags=0, autotune=False,
                  use_graph=True, tuner=None):
         N.load()
         self.patches = list(patches)

@@ -235,7 +235,7 @@ __host__ __device__ inline tile_smem tile_smem_layout(int tile_pixels, int max_g
 // tile kernel
 // ---------------------------------------------------------------------------
 template <int P>
-__global__ void __launch_bounds__(FP_THREADS, 3)
+__global__ void __launch_bounds__(FP_THREADS, 4)
 tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc *__restrict__ expos,
             const fp_tile *__restrict__ tiles, const int32_t *__restrict__ order,
             const int32_t *__restrict__ perm, int64_t n_tiles,

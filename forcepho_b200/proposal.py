@@ -77,7 +77,7 @@ class B200Proposer(ProposerBase):
     flags : extra ``fp_launch`` flags (e.g. ``FLAG_NO_CULL``).
     """
 
-    def __init__(self, patch=None, tile_pixels=None, ctas_per_sm=3, flags=0):
+    def __init__(self, patch=None, tile_pixels=None, ctas_per_sm=4, flags=0):
         N.load()
         self.patch = patch
         self.tile_pixels = tile_pixels

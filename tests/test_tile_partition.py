@@ -12,7 +12,7 @@ import itertools
 import pytest
 
 WARPS = 8
-CHUNK = 256
+CHUNK = 128
 SLOT_GROUPS = CHUNK // 32 + WARPS - 1
 
 
