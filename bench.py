@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "limits", "multiband", "small"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "limits", "multiband", "small", "hmc"])
+    ap.add_argument("--hmc-steps", type=int, default=16, help="leapfrog steps per trajectory (hmc workload)")
     ap.add_argument("--patches", type=int, default=512)
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
@@ -216,6 +217,42 @@ def cpu_tasks(args, rank, use_ref):
         for b in range(nb):
             tasks.append((kind, sh, b, use_ref))
     return tasks
+
+
+def cpu_precision(patches, proposals, results, n_check=3):
+    """Part of the CPU-baseline leg, untimed: the first ``n_check`` patches of the
+    timed batch, with the exact inputs the GPU saw, evaluated by the FP64
+    oracle and by the reference CPU kernel, compared with the batched GPU
+    results.  chi2 errors are given relative to |chi2| and to
+    sum (r^2 + d^2) ierr^2; gradient errors per parameter column, normwise."""
+    from oracle import oracle as O
+    # the first patches small enough for the single-threaded reference kernel
+    picked = [i for i, p in enumerate(patches) if p.n_pairs() <= 4e8][:n_check]
+    out = {"patches": picked, "vs_f64": {}, "vs_reference": {}}
+    worst = {"f64": [0.0, 0.0, 0.0], "ref": [0.0, 0.0, 0.0]}
+    for i in picked:
+        p, prop = patches[i], proposals[i]
+        c_g, g_g = results[i]
+        c64, g64, r64 = O.evaluate(p, prop, precision="f64", return_residual=True)
+        cref, gref, _ = O.ref_evaluate(p, prop)
+        for key, c, gg in (("f64", c64, g64), ("ref", cref, gref)):
+            for b in range(p.n_bands):
+                e0, ne = int(p.band_start[b]), int(p.band_N[b])
+                s0 = int(p.exposure_start[e0])
+                s1 = int(p.exposure_start[e0 + ne - 1] + p.exposure_N[e0 + ne - 1])
+                d = p.data[s0:s1].astype(np.float64) * p.ierr[s0:s1]
+                r = r64[s0:s1] * p.ierr[s0:s1]
+                sc = float(np.sum(d * d + r * r))
+                worst[key][0] = max(worst[key][0], abs(c_g[b] - c[b]) / max(abs(c[b]), 1e-300))
+                worst[key][1] = max(worst[key][1], abs(c_g[b] - c[b]) / sc)
+            for k in range(7):
+                den = np.linalg.norm(gg[..., k])
+                if den > 0:
+                    worst[key][2] = max(worst[key][2], float(np.linalg.norm(g_g[..., k] - gg[..., k]) / den))
+    for key, name in (("f64", "vs_f64"), ("ref", "vs_reference")):
+        out[name] = {"chi2_relerr_max": worst[key][0], "chi2_err_over_scale_max": worst[key][1],
+                     "grad_colnorm_relerr_max": worst[key][2]}
+    return out
 
 
 def cpu_measure(args, rank, seconds, cores=None):
@@ -455,9 +492,11 @@ def run_ours(args):
                  "max_chi2_diff_vs_batched": worst_c, "max_grad_normdiff_vs_batched": worst_g}
 
     cpu = None
+    precision = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_measure(args, rank, args.cpu_seconds)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        precision = cpu_precision(patches, proposals, bres)
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -470,6 +509,7 @@ def run_ours(args):
                                                                        % world}),
                "lnlike_grad_evals_per_s": total_patches / (ms_max * 1e-3),
                "e2e": e2e, "plain": plain_out, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+               "precision": precision,
                "gpu_launches": 3 * args.steps,
                "pairs": {"total": n_pairs, "evaluated_after_cull": evaluated, "within_cutoff": active,
                          "within_cutoff_but_culled": dropped},
@@ -480,10 +520,89 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+def run_hmc(args):
+    """Device-resident HMC on patches of the limits distribution (30 sources,
+    8 bands x 4 exposures of 256x256 px, 6-Gaussian PSFs): --patches of them
+    (128 unless given), --hmc-steps leapfrog steps per trajectory, --warmup
+    adapting trajectories, then --steps timed trajectories (CUDA-graph replays)."""
+    import torch
+    from forcepho_b200 import synthetic as S
+    from forcepho_b200.batch import render_models
+    from forcepho_b200.hmc import DeviceHMC
+    from forcepho_b200.proposal import B200Proposer
+    torch.cuda.set_device(0)
+    n = 128 if args.patches == 512 else args.patches
+    rng = np.random.default_rng(5)
+    t0 = time.perf_counter()
+    patches = [S.config_limits(seed=int(rng.integers(2 ** 31))) for _ in range(n)]
+    models = render_models(patches)
+    theta0 = []
+    for p, m in zip(patches, models):
+        r = np.random.default_rng(int(rng.integers(2 ** 31)))
+        S.add_noise(p, r, r.uniform(0.5, 2.0, p.n_exp), m)
+        p.return_residual = False
+        p.send_to_device()
+        th = p.scene.get_all_source_params().reshape(int(p.n_sources), -1).copy()
+        th[:, :p.n_bands] *= r.uniform(0.9, 1.1, th[:, :p.n_bands].shape)   # start off the truth
+        theta0.append(th.reshape(-1))
+    n_traj = args.warmup + args.steps + 2
+    h = DeviceHMC(patches, theta0, n_steps=args.hmc_steps, max_traj=n_traj, step_size=0.05)
+    h.estimate_inv_mass()
+    setup_s = time.perf_counter() - t0
+    h.run(args.warmup, adapt=True)
+    torch.cuda.synchronize()
+    acc0 = h.accepted.clone()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    props_dev = torch.cuda.get_device_properties(0)
+    gpu_id = ("GPU-" + str(props_dev.uuid)) if getattr(props_dev, "uuid", None) else "0"
+    with ClockSampler(gpu_id) as clk:
+        e0.record(stream)
+        h.run(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    grad_evals = n * args.hmc_steps * args.steps
+    pairs = h.plan.n_pairs * args.hmc_steps * args.steps
+    acc = ((h.accepted - acc0).double() / args.steps).cpu().numpy()
+    de = h.energy_error.cpu().numpy()
+    out = {"metric": METRIC, "value": pairs / (ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "hmc", "patches": n, "leapfrog_steps": args.hmc_steps,
+                      "patch": "30 sources, 8 bands x 4 exposures of 256x256 px, 6-Gaussian PSFs",
+                      "mass_matrix": "diagonal, Hessian-diagonal estimate (8 Hutchinson probes)",
+                      "step": "a trajectory of every patch (graph replay)"},
+           "gradient_evals_per_s": grad_evals / (ms * 1e-3),
+           "trajectories_per_s": n * args.steps / (ms * 1e-3),
+           "acceptance_mean": float(acc.mean()), "energy_error_abs_median": float(np.median(np.abs(de))),
+           "clocks": clk.summary(), "setup_s": setup_s, "gpu_launches": args.steps * (6 * args.hmc_steps + 2)}
+    if not args.no_cpu:
+        # CPU leg (checker, untimed): patch 0 at its final position vs the FP64
+        # oracle and the reference CPU kernel, two bands
+        from oracle import oracle as O
+        p = patches[0]
+        h.positions()                       # proposals at the current (accepted) positions
+        props = h.proposals()[0][:int(p.n_sources)].copy()
+        chi2, dchi2 = B200Proposer().evaluate_proposal(props, patch=p)
+        prec = {}
+        for name, fn in (("vs_f64", lambda: O.evaluate(p, props, precision="f64", bands=(0, 4))),
+                         ("vs_reference", lambda: O.ref_evaluate(p, props, bands=(0, 4)))):
+            c, g, _ = fn()
+            prec[name] = {"chi2_relerr_max": float(max(abs(chi2[b] - c[b]) / abs(c[b]) for b in (0, 4))),
+                          "grad_colnorm_relerr_max": float(max(
+                              np.linalg.norm(dchi2[b][..., k] - g[b][..., k]) / np.linalg.norm(g[b][..., k])
+                              for b in (0, 4) for k in range(7) if np.linalg.norm(g[b][..., k]) > 0))}
+        out["precision"] = dict(prec, patch=0, bands=[0, 4], state="final HMC position")
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "hmc":
+        run_hmc(args)
     else:
         run_ours(args)
 

@@ -112,22 +112,24 @@ def _proposal(proposal):
     return p, p.ctypes.data
 
 
-def evaluate(patch, proposal, precision="f32", return_residual=False, nthreads=None):
+def evaluate(patch, proposal, precision="f32", return_residual=False, nthreads=None, bands=None):
     """chi2[n_bands] (f64), dchi2[n_bands, n_sources, 7], residual or None.
 
     ``precision="f32"`` restates the reference arithmetic (dchi2 f32);
-    ``"f64"`` computes everything in FP64 (dchi2 f64, residual f64)."""
+    ``"f64"`` computes everything in FP64 (dchi2 f64, residual f64).
+    ``bands``: evaluate only these bands (the others are left zero)."""
     L = lib()
     nb, ns = patch.n_bands, int(patch.n_sources)
+    todo = range(nb) if bands is None else list(bands)
     if nthreads is None:
-        nthreads = min(os.cpu_count() or 1, 8)
+        nthreads = min(os.cpu_count() or 1, 32)
     prop, pptr = _proposal(proposal)
     chi2 = np.zeros(nb, dtype=np.float64)
     if precision == "f32":
         res = np.zeros(patch.npix, dtype=np.float32) if return_residual else None
         hs = HostStruct(patch, residual=res)
         grads = np.zeros((nb, MAXSOURCES * NPARAMS), dtype=np.float32)
-        for b in range(nb):
+        for b in todo:
             c = ctypes.c_double()
             rc = L.fpo_evaluate_band_f32(hs.ptr, pptr, b, ctypes.addressof(c),
                                          grads[b].ctypes.data, nthreads)
@@ -138,7 +140,7 @@ def evaluate(patch, proposal, precision="f32", return_residual=False, nthreads=N
         hs = HostStruct(patch)
         res = np.zeros(patch.npix, dtype=np.float64) if return_residual else None
         grads = np.zeros((nb, MAXSOURCES * NPARAMS), dtype=np.float64)
-        for b in range(nb):
+        for b in todo:
             c = ctypes.c_double()
             rc = L.fpo_evaluate_band_f64(hs.ptr, pptr, b, ctypes.addressof(c),
                                          grads[b].ctypes.data,
@@ -152,8 +154,9 @@ def evaluate(patch, proposal, precision="f32", return_residual=False, nthreads=N
     return chi2, dchi2, res
 
 
-def ref_evaluate(patch, proposal, return_residual=False):
-    """The reference CPU kernel, one pybind call per band (CPUProposer's loop)."""
+def ref_evaluate(patch, proposal, return_residual=False, bands=None):
+    """The reference CPU kernel, one pybind call per band (CPUProposer's loop);
+    ``bands``: only these bands (the others are left zero)."""
     mod = ref_module()
     nb, ns = patch.n_bands, int(patch.n_sources)
     res = np.zeros(patch.npix, dtype=np.float32) if return_residual else None
@@ -161,7 +164,7 @@ def ref_evaluate(patch, proposal, return_residual=False):
     prop, pptr = _proposal(proposal)
     chi2 = np.zeros(nb, dtype=np.float64)
     dchi2 = np.zeros((nb, ns, NPARAMS), dtype=np.float32)
-    for b in range(nb):
+    for b in (range(nb) if bands is None else bands):
         r = mod.EvaluateProposal(b, hs.ptr, pptr)
         chi2[b] = r.chi2
         dchi2[b] = np.asarray(r.dchi2_dp).reshape(MAXSOURCES, NPARAMS)[:ns]

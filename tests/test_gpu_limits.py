@@ -1,0 +1,97 @@
+"""The limits workload on the GPU: 30 sources, 8 bands x 4 exposures of
+256x256 pixels, 6-Gaussian PSFs (1620 image Gaussians per exposure, 2.1 M
+pixels).  The CPU checkers are run on a subset of bands (each band is an
+independent output of the kernel), which keeps them to seconds."""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tolerances import CHI2_F64, CHI2_REF, GRAD_F64, GRAD_REF, chi2_err, grad_err
+
+pytestmark = pytest.mark.gpu
+
+BANDS = (0, 5)
+
+
+@pytest.fixture(scope="module")
+def limits_patch():
+    from forcepho_b200 import synthetic as S
+    from forcepho_b200.batch import render_models
+    p = S.config_limits(seed=3)
+    rng = np.random.default_rng(31)
+    model = render_models([p])[0]
+    S.add_noise(p, rng, rng.uniform(0.5, 2.0, p.n_exp), model)
+    p.return_residual = True
+    p.send_to_device()
+    th = p.scene.get_all_source_params().reshape(30, -1)
+    th[:, 8] *= 1.0 + rng.normal(0, 1e-7, 30)            # ra, dec off the truth
+    th[:, 9] += rng.normal(0, 1e-6, 30)
+    th[:, 10] = np.clip(th[:, 10] * 0.97, 0.2, 0.99)      # q
+    p.scene.set_all_source_params(th.reshape(-1))
+    return p, p.scene.get_proposal().copy()
+
+
+def band_scale(p, res, b):
+    e0, ne = int(p.band_start[b]), int(p.band_N[b])
+    s0 = int(p.exposure_start[e0])
+    s1 = int(p.exposure_start[e0 + ne - 1] + p.exposure_N[e0 + ne - 1])
+    d = p.data[s0:s1].astype(np.float64) * p.ierr[s0:s1]
+    r = np.asarray(res[s0:s1], np.float64) * p.ierr[s0:s1]
+    return float(np.sum(d * d + r * r))
+
+
+@pytest.mark.parametrize("kind", ["tiled", "plain"])
+def test_limits_parity(limits_patch, kind):
+    from forcepho_b200.proposal import B200Proposer, PlainProposer
+    p, prop = limits_patch
+    assert p.max_gauss_per_exposure() == 1620 and p.npix == 32 * 65536
+    chi2, dchi2, res = (B200Proposer() if kind == "tiled" else PlainProposer()).evaluate_proposal(
+        prop, patch=p, unpack=False)
+    c64, g64, _ = O.evaluate(p, prop, precision="f64", bands=BANDS)
+    cref, gref, _ = O.ref_evaluate(p, prop, bands=BANDS)
+    for b in BANDS:
+        sc = band_scale(p, res, b)
+        e64 = abs(chi2[b] - c64[b]) / sc
+        eref = abs(chi2[b] - cref[b]) / sc
+        g64e = grad_err(dchi2[b], g64[b])
+        grefe = grad_err(dchi2[b], gref[b])
+        assert eref < CHI2_REF and grefe < GRAD_REF, (kind, b, eref, grefe)
+        if kind == "tiled":
+            assert e64 < CHI2_F64 and g64e < GRAD_F64, (kind, b, e64, g64e)
+            # the precision claim: relative error against chi2 itself too
+            assert abs(chi2[b] - c64[b]) / abs(c64[b]) < 1e-6, (b, chi2[b], c64[b])
+
+
+def test_limits_autograd_and_fd(limits_patch):
+    """PatchChi2 at 420 parameters; backward against central differences of
+    the FP64 oracle's chi2 of one band, for every parameter of two sources."""
+    import torch
+    from forcepho_b200.autograd import PatchChi2
+    p, prop = limits_patch
+    p.return_residual = False
+    th0 = p.scene.get_all_source_params().astype(np.float32).astype(np.float64)
+    fn = PatchChi2(p)
+    theta = torch.tensor(th0, dtype=torch.float64, device="cuda", requires_grad=True)
+    w = torch.zeros(p.n_bands, dtype=torch.float64, device="cuda")
+    b = BANDS[1]
+    w[b] = 1.0
+    (fn(theta) * w).sum().backward()
+    g = theta.grad.cpu().numpy().reshape(30, 14)
+    steps = [2.0 ** -10, 2.0 ** -30, 2.0 ** -30, 2.0 ** -14, 2.0 ** -14, 2.0 ** -7, 2.0 ** -12]
+
+    def chi2_b(th):
+        p.scene.set_all_source_params(th)
+        return O.evaluate(p, p.scene.get_proposal(), precision="f64", bands=[b])[0][b]
+
+    for s in (3, 17):
+        cols = [b] + list(range(8, 14))     # this band's flux, then ra..rhalf
+        for k, col in enumerate(cols):
+            h = steps[k]
+            tp, tm = th0.copy(), th0.copy()
+            tp[s * 14 + col] += h
+            tm[s * 14 + col] -= h
+            fd = (chi2_b(tp) - chi2_b(tm)) / (2 * h)
+            an = g[s, col]
+            assert abs(an - fd) <= 2e-3 * abs(fd) + 1e-6 * np.abs(g).max(), (s, col, an, fd)
+    p.scene.set_all_source_params(th0)
