@@ -33,6 +33,7 @@
 namespace {
 
 constexpr int SLOT_GROUPS = FP_CHUNK / 32 + FP_WARPS - 1;   // adjoint result slots per lane
+static_assert(FP_CHUNK / 32 <= 16, "adjoint group warp masks live in s_int[16..32)");
 
 // ---------------------------------------------------------------------------
 // setup
@@ -253,7 +254,8 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
     double *s_slot = reinterpret_cast<double *>(smem + L.slot);
     double *s_src = reinterpret_cast<double *>(smem + L.src);
     double *s_red = reinterpret_cast<double *>(smem + L.red);
-    int *s_int = reinterpret_cast<int *>(smem + L.ints);          // [0] item, [8..16) warp counts
+    int *s_int = reinterpret_cast<int *>(smem + L.ints);          // [0] item, [8..16) warp counts,
+                                                                    // [16..20) adjoint group warp masks
     uint16_t *s_idx = reinterpret_cast<uint16_t *>(smem + L.idx);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -453,13 +455,24 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
                     s_gb[i] = gfwd[2 * gi + 1];
                 }
             }
-            for (int i = tid; i < SLOT_GROUPS * 32 * NPARAMS; i += FP_THREADS) s_slot[i] = 0.0;
-            __syncthreads();
-
             // the (group of 32 Gaussians) x (pixel) plane, split evenly over the warps;
-            // warp w writes its segment of group g into slot group g + w
+            // warp w writes its segment of group g into slot group g + w.  Bit w of
+            // s_int[16 + g] says whether warp w's share [W w/8, W (w+1)/8) meets the
+            // row of group g, i.e. whether slot group g + w holds a part of group g
+            // (every slot read below was written in this chunk: no zeroing needed)
             const int ngrp = (cn + 31) >> 5;
             const int64_t W = (int64_t)ngrp * nzt;
+            if (tid < ngrp) {
+                const int64_t r0 = (int64_t)tid * nzt, r1 = r0 + nzt;
+                int mask = 0;
+#pragma unroll
+                for (int w = 0; w < FP_WARPS; ++w) {
+                    const int64_t a = W * w / FP_WARPS, b = W * (w + 1) / FP_WARPS;
+                    if (a < b && a < r1 && b > r0) mask |= 1 << w;
+                }
+                s_int[16 + tid] = mask;
+            }
+            __syncthreads();
             int64_t u = W * warp / FP_WARPS;
             const int64_t u1 = W * (warp + 1) / FP_WARPS;
             while (u < u1) {
@@ -486,29 +499,28 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
             }
             __syncthreads();
 
-            // per-source sums over this chunk, fixed order (Gaussian, then warp)
+            // per-source sums over this chunk, fixed order (Gaussian, then warp).
+            // Gaussian g belongs to source g / n_psf; the chunk's Gaussians ascend, so
+            // source s owns the run of entries with s n_psf <= g < (s + 1) n_psf
             for (int t = tid; t < ns * NPARAMS; t += FP_THREADS) {
                 const int s = t / NPARAMS, k = t - s * NPARAMS;
+                const int key0 = s * n_psf, key1 = key0 + n_psf;
                 int lo = 0, hi = cn;
                 while (lo < hi) {
                     const int mid = (lo + hi) >> 1;
-                    if ((int)s_idx[c0 + mid] / n_psf < s) lo = mid + 1; else hi = mid;
+                    if ((int)s_idx[c0 + mid] < key0) lo = mid + 1; else hi = mid;
                 }
                 int end = lo, hi2 = cn;
                 while (end < hi2) {
                     const int mid = (end + hi2) >> 1;
-                    if ((int)s_idx[c0 + mid] / n_psf <= s) end = mid + 1; else hi2 = mid;
+                    if ((int)s_idx[c0 + mid] < key1) end = mid + 1; else hi2 = mid;
                 }
                 double acc = 0.0;
                 for (int gl = lo; gl < end; ++gl) {
                     const int grp = gl >> 5, ln = gl & 31;
-                    // slot group grp + w holds warp w's segment of group grp only if
-                    // warp w's share [W w/8, W (w+1)/8) of the plane meets this group's row
-                    const int64_t r0 = (int64_t)grp * nzt, r1 = r0 + nzt;
-#pragma unroll
-                    for (int w = 0; w < FP_WARPS; ++w) {
-                        const int64_t a = W * w / FP_WARPS, b = W * (w + 1) / FP_WARPS;
-                        if (a < b && a < r1 && b > r0) acc += s_slot[((size_t)(grp + w) * 32 + ln) * NPARAMS + k];
+                    for (unsigned m = (unsigned)s_int[16 + grp]; m != 0u; m &= m - 1u) {
+                        const int w = __ffs(m) - 1;
+                        acc += s_slot[((size_t)(grp + w) * 32 + ln) * NPARAMS + k];
                     }
                 }
                 s_src[t] += acc;
