@@ -32,8 +32,6 @@
 
 namespace {
 
-constexpr int SLOT_GROUPS = FP_CHUNK / 32 + FP_WARPS - 1;   // adjoint result slots per lane
-static_assert(FP_CHUNK / 32 <= 16, "adjoint group warp masks live in s_int[16..32)");
 
 // ---------------------------------------------------------------------------
 // setup
@@ -212,7 +210,7 @@ __device__ __forceinline__ bool ellipse_meets_rect(const float4 A, float fys, fl
 }
 
 struct tile_smem {
-    size_t ga, gb, box, pix, slot, src, red, ints, idx, total;
+    size_t ga, gb, box, pix, wsrc, red, ints, idx, total;
 };
 
 __host__ __device__ inline tile_smem tile_smem_layout(int tile_pixels, int max_gauss)
@@ -223,8 +221,7 @@ __host__ __device__ inline tile_smem tile_smem_layout(int tile_pixels, int max_g
     L.gb = o;   o += (size_t)FP_CHUNK * 16;
     L.box = o;  o += (size_t)FP_CHUNK * 16;
     L.pix = o;  o += (size_t)tile_pixels * 16;
-    L.slot = o; o += (size_t)SLOT_GROUPS * 32 * NPARAMS * 8;
-    L.src = o;  o += (size_t)MAXSOURCES * NPARAMS * 8;
+    L.wsrc = o; o += (size_t)FP_WARPS * MAXSOURCES * NPARAMS * 8;
     L.red = o;  o += 16 * 8;
     L.ints = o; o += 32 * 4;
     L.idx = o;  o += ((size_t)max_gauss * 2 + 15) & ~(size_t)15;
@@ -251,11 +248,11 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
     float4 *s_gb = reinterpret_cast<float4 *>(smem + L.gb);
     float4 *s_gbox = reinterpret_cast<float4 *>(smem + L.box);
     float4 *s_pix = reinterpret_cast<float4 *>(smem + L.pix);
-    double *s_slot = reinterpret_cast<double *>(smem + L.slot);
-    double *s_src = reinterpret_cast<double *>(smem + L.src);
+    // per-warp source gradients [warp][source][param]: each warp adds its own
+    // results into its own row, in its own program order
+    double *s_wsrc = reinterpret_cast<double *>(smem + L.wsrc);
     double *s_red = reinterpret_cast<double *>(smem + L.red);
-    int *s_int = reinterpret_cast<int *>(smem + L.ints);          // [0] item, [8..16) warp counts,
-                                                                    // [16..20) adjoint group warp masks
+    int *s_int = reinterpret_cast<int *>(smem + L.ints);          // [0] item, [8..16) warp counts
     uint16_t *s_idx = reinterpret_cast<uint16_t *>(smem + L.idx);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -442,7 +439,7 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
             for (int w = 0; w < FP_WARPS; ++w) t += s_red[w];
             s_red[FP_WARPS] = t;
         }
-        for (int t = tid; t < MAXSOURCES * NPARAMS; t += FP_THREADS) s_src[t] = 0.0;
+        for (int t = tid; t < FP_WARPS * MAXSOURCES * NPARAMS; t += FP_THREADS) s_wsrc[t] = 0.0;
 
         // ---- 3. adjoint: one Gaussian per lane, pixels broadcast ----
         for (int c0 = 0; c0 < gc; c0 += FP_CHUNK) {
@@ -455,24 +452,10 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
                     s_gb[i] = gfwd[2 * gi + 1];
                 }
             }
-            // the (group of 32 Gaussians) x (pixel) plane, split evenly over the warps;
-            // warp w writes its segment of group g into slot group g + w.  Bit w of
-            // s_int[16 + g] says whether warp w's share [W w/8, W (w+1)/8) meets the
-            // row of group g, i.e. whether slot group g + w holds a part of group g
-            // (every slot read below was written in this chunk: no zeroing needed)
+            // the (group of 32 Gaussians) x (pixel) plane, split evenly over the warps
+            __syncthreads();
             const int ngrp = (cn + 31) >> 5;
             const int64_t W = (int64_t)ngrp * nzt;
-            if (tid < ngrp) {
-                const int64_t r0 = (int64_t)tid * nzt, r1 = r0 + nzt;
-                int mask = 0;
-#pragma unroll
-                for (int w = 0; w < FP_WARPS; ++w) {
-                    const int64_t a = W * w / FP_WARPS, b = W * (w + 1) / FP_WARPS;
-                    if (a < b && a < r1 && b > r0) mask |= 1 << w;
-                }
-                s_int[16 + tid] = mask;
-            }
-            __syncthreads();
             int64_t u = W * warp / FP_WARPS;
             const int64_t u1 = W * (warp + 1) / FP_WARPS;
             while (u < u1) {
@@ -487,50 +470,49 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
 #pragma unroll
                 for (int k = 0; k < 12; ++k) mom[k] = 0.0;
                 adjoint_moments(A, B, s_pix, p0, p1, mom);
+                double g7[NPARAMS];
+                int src = -1;
                 if (valid) {
-                    const int64_t gi = ed.gauss_offset + s_idx[c0 + gl];
-                    double g7[NPARAMS];
-                    moments_to_grad(gjac + (size_t)FP_JAC * gi, mom, g7);
-                    double *slot = s_slot + ((size_t)(grp + warp) * 32 + lane) * NPARAMS;
+                    const int gidx = s_idx[c0 + gl];
+                    moments_to_grad(gjac + (size_t)FP_JAC * (ed.gauss_offset + gidx), mom, g7);
+                    src = gidx / n_psf;               // Gaussian g belongs to source g / n_psf
+                } else {
 #pragma unroll
-                    for (int k = 0; k < NPARAMS; ++k) slot[k] = g7[k];
+                    for (int k = 0; k < NPARAMS; ++k) g7[k] = 0.0;
                 }
-                u += p1 - p0;
-            }
-            __syncthreads();
-
-            // per-source sums over this chunk, fixed order (Gaussian, then warp).
-            // Gaussian g belongs to source g / n_psf; the chunk's Gaussians ascend, so
-            // source s owns the run of entries with s n_psf <= g < (s + 1) n_psf
-            for (int t = tid; t < ns * NPARAMS; t += FP_THREADS) {
-                const int s = t / NPARAMS, k = t - s * NPARAMS;
-                const int key0 = s * n_psf, key1 = key0 + n_psf;
-                int lo = 0, hi = cn;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if ((int)s_idx[c0 + mid] < key0) lo = mid + 1; else hi = mid;
-                }
-                int end = lo, hi2 = cn;
-                while (end < hi2) {
-                    const int mid = (end + hi2) >> 1;
-                    if ((int)s_idx[c0 + mid] < key1) end = mid + 1; else hi2 = mid;
-                }
-                double acc = 0.0;
-                for (int gl = lo; gl < end; ++gl) {
-                    const int grp = gl >> 5, ln = gl & 31;
-                    for (unsigned m = (unsigned)s_int[16 + grp]; m != 0u; m &= m - 1u) {
-                        const int w = __ffs(m) - 1;
-                        acc += s_slot[((size_t)(grp + w) * 32 + ln) * NPARAMS + k];
+                // segmented sum over the lanes of each source: the chunk's Gaussians
+                // ascend, so a source's lanes are contiguous; after the fixed
+                // shuffle tree the first lane of each source holds its sum
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int so = __shfl_down_sync(0xffffffffu, src, o);
+                    const bool same = (lane + o < 32) && (so == src);
+#pragma unroll
+                    for (int k = 0; k < NPARAMS; ++k) {
+                        const double v = __shfl_down_sync(0xffffffffu, g7[k], o);
+                        if (same) g7[k] += v;
                     }
                 }
-                s_src[t] += acc;
+                const int sprev = __shfl_up_sync(0xffffffffu, src, 1);
+                if (valid && (lane == 0 || sprev != src)) {
+                    double *row = s_wsrc + ((size_t)warp * MAXSOURCES + src) * NPARAMS;
+#pragma unroll
+                    for (int k = 0; k < NPARAMS; ++k) row[k] += g7[k];
+                }
+                __syncwarp();   // another lane may update the same row in the next segment
+                u += p1 - p0;
             }
         }
         __syncthreads();
 
         // ---- 4. per-tile partials ----
         if (tid == 0) out[0] = s_red[FP_WARPS];
-        for (int t = tid; t < ns * NPARAMS; t += FP_THREADS) out[1 + t] = s_src[t];
+        for (int t = tid; t < ns * NPARAMS; t += FP_THREADS) {
+            double acc = 0.0;
+#pragma unroll
+            for (int w = 0; w < FP_WARPS; ++w) acc += s_wsrc[(size_t)w * MAXSOURCES * NPARAMS + t];
+            out[1 + t] = acc;
+        }
         // the next iteration's first barrier orders these reads before any reuse
     }
 }

@@ -1,98 +1,97 @@
 """CPU replay of the tile kernel's adjoint work partition (forcepho_b200/csrc/tiled.cu).
 
 The (group of 32 Gaussians) x (nonzero pixel) plane of one chunk is split
-evenly over the 8 warps; warp w writes its segment of group g into slot group
-g + w, and the per-source reduction sums, for group g, the slot groups g + w
-of exactly the warps whose share meets row g (a bit mask per group, computed
-once per chunk).  This replays that integer arithmetic and checks that every
-(group, pixel) unit is summed exactly once, that no two segments share a slot
-(so every slot read was written in the same chunk), and that the source ranges
-found without integer division are the ones division gives."""
+evenly over the 8 warps; a warp walks its share as segments, one per group
+row it meets.  After each segment the warp sums its lanes' gradients per
+source with a segmented shuffle tree (a source's Gaussians occupy contiguous
+lanes, invalid lanes carry source -1) and the first lane of each source adds
+the sum into the warp's own row of per-source gradients; the rows of the 8
+warps are summed once per tile.  This replays that integer arithmetic and
+checks that every (group, pixel) unit is processed exactly once and that the
+shuffle tree leaves each source's exact sum on its first lane."""
 
 import itertools
 
+import numpy as np
 import pytest
 
 WARPS = 8
 CHUNK = 128
-SLOT_GROUPS = CHUNK // 32 + WARPS - 1
 
 
 def segments(ngrp, nzt):
     W = ngrp * nzt
-    segs = []      # (warp, group, p0, p1, slot)
+    segs = []      # (warp, group, p0, p1)
     for w in range(WARPS):
         u, u1 = W * w // WARPS, W * (w + 1) // WARPS
         while u < u1:
             grp = u // nzt
             p0 = u - grp * nzt
             p1 = min(nzt, p0 + (u1 - u))
-            segs.append((w, grp, p0, p1, grp + w))
+            segs.append((w, grp, p0, p1))
             u += p1 - p0
     return segs
-
-
-def group_mask(ngrp, nzt, grp):
-    W = ngrp * nzt
-    r0, r1 = grp * nzt, grp * nzt + nzt
-    mask = 0
-    for w in range(WARPS):
-        a, b = W * w // WARPS, W * (w + 1) // WARPS
-        if a < b and a < r1 and b > r0:
-            mask |= 1 << w
-    return mask
-
-
-def reader_slots(ngrp, nzt, grp):
-    m = group_mask(ngrp, nzt, grp)
-    out = []
-    while m:                                    # lowest set bit first, as __ffs
-        w = (m & -m).bit_length() - 1
-        m &= m - 1
-        out.append(grp + w)
-    return out
 
 
 @pytest.mark.parametrize("ngrp,nzt", list(itertools.product(range(1, CHUNK // 32 + 1),
                                                             [1, 2, 3, 7, 8, 31, 32, 33, 100, 255, 256,
                                                              257, 511, 1000, 1023, 1024])))
 def test_partition_covers_plane_once(ngrp, nzt):
-    segs = segments(ngrp, nzt)
-    slots = [s[4] for s in segs]
-    assert len(slots) == len(set(slots)), "two segments share a slot"
-    assert max(slots) < SLOT_GROUPS
-    by_slot = {s[4]: s for s in segs}
+    covered = {g: [] for g in range(ngrp)}
+    for w, grp, p0, p1 in segments(ngrp, nzt):
+        assert 0 <= p0 < p1 <= nzt
+        covered[grp].extend(range(p0, p1))
     for g in range(ngrp):
-        covered = []
-        for sl in reader_slots(ngrp, nzt, g):
-            w, grp, p0, p1, _ = by_slot[sl]
-            assert grp == g, "reader takes another group's segment"
-            covered.extend(range(p0, p1))
-        assert sorted(covered) == list(range(nzt))
+        assert sorted(covered[g]) == list(range(nzt))
 
 
-def _search(keys, lo, hi, pred):
-    while lo < hi:
-        mid = (lo + hi) >> 1
-        if pred(keys[mid]):
-            lo = mid + 1
-        else:
-            hi = mid
-    return lo
+def segmented_lane_sums(src, val):
+    """The kernel's shuffle tree: lane l adds lane l+o's value (read before this
+    step) when l+o < 32 and both lanes hold the same source."""
+    v = list(val)
+    for o in (1, 2, 4, 8, 16):
+        prev = list(v)
+        for lane in range(32):
+            if lane + o < 32 and src[lane + o] == src[lane]:
+                v[lane] = prev[lane] + prev[lane + o]
+    heads = {}
+    for lane in range(32):
+        if src[lane] >= 0 and (lane == 0 or src[lane - 1] != src[lane]):
+            heads[src[lane]] = v[lane]
+    return heads
 
 
-@pytest.mark.parametrize("n_psf", [1, 3, 4, 36, 40])
-def test_source_ranges_without_division(n_psf):
-    import numpy as np
-    rng = np.random.default_rng(n_psf)
-    for _ in range(50):
-        ns = int(rng.integers(1, 31))
-        kept = np.sort(rng.choice(ns * n_psf, size=int(rng.integers(1, min(CHUNK, ns * n_psf) + 1)),
-                                  replace=False))
-        for s in range(ns):
-            lo_div = _search(kept, 0, len(kept), lambda g: g // n_psf < s)
-            end_div = _search(kept, lo_div, len(kept), lambda g: g // n_psf <= s)
-            lo = _search(kept, 0, len(kept), lambda g: g < s * n_psf)
-            end = _search(kept, lo, len(kept), lambda g: g < (s + 1) * n_psf)
-            assert (lo, end) == (lo_div, end_div)
-            assert all(g // n_psf == s for g in kept[lo:end])
+@pytest.mark.parametrize("seed", range(40))
+def test_segmented_shuffle_sums(seed):
+    rng = np.random.default_rng(seed)
+    n_valid = int(rng.integers(1, 33))
+    # ascending sources over the valid lanes, -1 on the rest
+    src = sorted(int(s) for s in rng.integers(0, int(rng.integers(1, 31)), n_valid)) + [-1] * (32 - n_valid)
+    val = [int(x) for x in rng.integers(-1000, 1000, 32)]
+    heads = segmented_lane_sums(src, val)
+    want = {}
+    for s, x in zip(src, val):
+        if s >= 0:
+            want[s] = want.get(s, 0) + x
+    assert heads == want
+
+
+@pytest.mark.parametrize("ngrp,nzt,n_psf", [(1, 5, 4), (2, 300, 36), (4, 1024, 36), (3, 33, 7), (4, 1, 36)])
+def test_every_unit_reaches_its_source_once(ngrp, nzt, n_psf):
+    """Integer stand-ins for the per-(Gaussian, pixel) gradient terms: the per-warp
+    source rows, summed over warps, equal the direct per-source sums."""
+    rng = np.random.default_rng(ngrp * 1000 + nzt)
+    cn = min(CHUNK, ngrp * 32 - int(rng.integers(0, 32)))
+    cn = max(cn, (ngrp - 1) * 32 + 1)
+    gidx = np.sort(rng.choice(30 * n_psf, size=cn, replace=False))
+    term = rng.integers(-50, 50, size=(cn, nzt))
+    rows = np.zeros((WARPS, 30), dtype=np.int64)
+    for w, grp, p0, p1 in segments(ngrp, nzt):
+        src = [int(gidx[grp * 32 + l]) // n_psf if grp * 32 + l < cn else -1 for l in range(32)]
+        val = [int(term[grp * 32 + l, p0:p1].sum()) if grp * 32 + l < cn else 0 for l in range(32)]
+        for s, x in segmented_lane_sums(src, val).items():
+            rows[w, s] += x
+    want = np.zeros(30, dtype=np.int64)
+    for i in range(cn):
+        want[gidx[i] // n_psf] += term[i].sum()
+    np.testing.assert_array_equal(rows.sum(axis=0), want)
