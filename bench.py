@@ -400,8 +400,10 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier()
         ev0.record(stream)
+        torch.cuda.nvtx.range_push("bench_timed")     # lets ncu --nvtx-include select the timed steps
         for _ in range(args.steps):
             bp.run(stream)
+        torch.cuda.nvtx.range_pop()
         ev1.record(stream)
         ev1.synchronize()
         torch.cuda.synchronize()
@@ -420,8 +422,10 @@ def run_ours(args):
         bp.plan.evaluate(lp_tiles, stream=stream)
     k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     k0.record(stream)
+    torch.cuda.nvtx.range_push("bench_tile_kernel")
     for _ in range(args.steps):
         bp.plan.evaluate(lp_tiles, stream=stream)
+    torch.cuda.nvtx.range_pop()
     k1.record(stream)
     k1.synchronize()
     tile_ms = k0.elapsed_time(k1) / args.steps
@@ -444,8 +448,10 @@ def run_ours(args):
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    torch.cuda.nvtx.range_push("bench_e2e")
     for _ in range(args.steps):
         res = bp.evaluate_proposals(proposals)
+    torch.cuda.nvtx.range_pop()
     e1.record(stream)
     e1.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)

@@ -22,7 +22,7 @@ int fp_sm_count(int *out);
 
 #define FP_THREADS 256              // threads per tile CTA
 #define FP_WARPS (FP_THREADS / 32)
-#define FP_CHUNK 128                // Gaussians staged in shared memory at a time
+#define FP_CHUNK 256                // Gaussians staged in shared memory at a time
 #define FP_RUN 32                   // FP32 run length before flushing to FP64
 
 // ---- device status word bits ----------------------------------------------

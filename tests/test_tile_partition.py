@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 WARPS = 8
-CHUNK = 128
+CHUNK = 256
 
 
 def segments(ngrp, nzt):
