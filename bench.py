@@ -42,6 +42,14 @@ FLOPS_PER_PAIR = 84      # FP32 flops (FMA = 2) of one forward + adjoint pair ev
 EX2_PER_PAIR = 2
 
 
+# DRAM bytes (read + write) of one tile_kernel launch, measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum, one pass, first timed launch of
+# "bench.py --steps 1 --warmup 3 --no-cpu --no-autotune --tile-pixels 1024"):
+# 6.00 GB read + 0.221 GB written.  Keyed by (workload, patches, tile pixels);
+# other configurations report null.
+TILE_TRAFFIC = {("batched", 512, 1024): 6.00e9 + 220.83e6}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -431,7 +439,8 @@ def run_ours(args):
     tile_ms = k0.elapsed_time(k1) / args.steps
     achieved = FLOPS_PER_PAIR * active / (tile_ms * 1e-3) / 1e12
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_tflops.value, "unit": "TFLOP/s",
-                "frac": achieved / fp32_tflops.value, "traffic": None,
+                "frac": achieved / fp32_tflops.value,
+                "traffic": TILE_TRAFFIC.get((args.workload, args.patches, bp.tile_pixels)),
                 "kernel": "tile_kernel<%d>" % (bp.tile_pixels // 256),
                 "kernel_ms": tile_ms, "share_of_step": tile_ms / ms,
                 "peak_source": "measured in this run: FFMA-chain kernel (fp_measure_peaks), not in MEASURED_PEAKS.json",
