@@ -20,11 +20,15 @@ import torch
 
 from . import _native as N
 from .autotune import Autotuner, size_class
-from .device import Plan, pack_proposals, response_view
+from .device import Plan, pack_proposals
 from .kernel_limits import MAXBANDS, MAXSOURCES, NPARAMS
 from .structs import source_struct_dtype
 
 __all__ = ["BatchedProposer", "render_models"]
+
+# a source record as raw bytes, for plain copies into the pinned staging buffer
+_RECORD = np.dtype("V%d" % source_struct_dtype.itemsize)
+_ZERO_RECORD = np.zeros(1, dtype=source_struct_dtype).view(_RECORD)[0]
 
 
 class BatchedProposer:
@@ -53,9 +57,29 @@ class BatchedProposer:
         else:
             self.plan = Plan(self.patches, tile_pixels=tile_pixels)
             self.launch = self.plan.launch(ctas_per_sm=ctas_per_sm, flags=flags)
+        self._init_host_buffers()
+
+    def _init_host_buffers(self):
+        """Pinned staging for proposals and compact results.
+
+        Proposals: the device layout, [n_patches][MAXSOURCES] records, written
+        patch by patch as raw 264-byte records; a slot left over from a longer
+        earlier proposal is zeroed.  Results: only the (patch, band) rows that
+        exist are gathered on the device and copied back (chi2 and Response
+        records), in patch-major, band-minor order."""
+        dev = self.plan.device
         self._pin_prop = torch.zeros(self.plan.proposals.numel(), dtype=torch.uint8).pin_memory()
-        self._pin_chi2 = torch.zeros(self.plan.chi2.shape, dtype=torch.float64).pin_memory()
-        self._pin_resp = torch.zeros(self.plan.response.shape, dtype=torch.float32).pin_memory()
+        self._prop_slots = self._pin_prop.numpy().view(_RECORD).reshape(self.n, MAXSOURCES)
+        self._prop_len = [0] * self.n
+        nb = [int(p.n_bands) for p in self.patches]
+        rows = [i * MAXBANDS + b for i in range(self.n) for b in range(nb[i])]
+        self._rows = torch.tensor(rows, dtype=torch.int64, device=dev)
+        self._dev_chi2 = torch.zeros(len(rows), dtype=torch.float64, device=dev)
+        self._dev_resp = torch.zeros((len(rows), MAXSOURCES * NPARAMS), dtype=torch.float32, device=dev)
+        self._pin_chi2 = torch.zeros(len(rows), dtype=torch.float64).pin_memory()
+        self._pin_resp = torch.zeros((len(rows), MAXSOURCES * NPARAMS), dtype=torch.float32).pin_memory()
+        offsets = np.concatenate([[0], np.cumsum(nb)[:-1]]).astype(int)
+        self._slices = [(int(o), nb[i], int(self.patches[i].n_sources)) for i, o in enumerate(offsets)]
 
     # --- launch parameters ---
     def _autotune(self, tuner):
@@ -89,9 +113,27 @@ class BatchedProposer:
 
     # --- device-side pieces (no host synchronisation) ---
     def set_proposals_async(self, proposals, stream=None):
-        """Stage host proposals (list of arrays) and queue their copy to the device."""
-        host = pack_proposals(proposals, self.n)
-        self._pin_prop.numpy()[:] = host.view(np.uint8).reshape(-1)
+        """Stage host proposals (list of ``source_struct_dtype`` arrays, one per
+        patch; patches past the end of the list get no sources) and queue
+        their copy to the device."""
+        if len(proposals) > self.n:
+            raise ValueError("%d proposals for %d patches" % (len(proposals), self.n))
+        slots, lens = self._prop_slots, self._prop_len
+        for i in range(self.n):
+            if i < len(proposals):
+                p = np.asarray(proposals[i])
+                if p.dtype != source_struct_dtype:
+                    p = p.astype(source_struct_dtype)
+                p = np.ascontiguousarray(p).reshape(-1)
+                k = len(p)
+                if k > MAXSOURCES:
+                    raise ValueError("proposal %d has %d sources > MAXSOURCES=%d" % (i, k, MAXSOURCES))
+                slots[i, :k] = p.view(_RECORD)
+            else:
+                k = 0
+            if k < lens[i]:
+                slots[i, k:lens[i]] = _ZERO_RECORD
+            lens[i] = k
         s = stream or torch.cuda.current_stream()
         with torch.cuda.stream(s):
             self.plan.proposals.copy_(self._pin_prop, non_blocking=True)
@@ -120,19 +162,23 @@ class BatchedProposer:
         return g
 
     def fetch_async(self, stream=None):
+        """Queue the device gather of the existing (patch, band) rows and their
+        copy into pinned host memory."""
         s = stream or torch.cuda.current_stream()
         with torch.cuda.stream(s):
-            self._pin_chi2.copy_(self.plan.chi2, non_blocking=True)
-            self._pin_resp.copy_(self.plan.response, non_blocking=True)
+            torch.index_select(self.plan.chi2.view(-1), 0, self._rows, out=self._dev_chi2)
+            torch.index_select(self.plan.response.view(-1, MAXSOURCES * NPARAMS), 0, self._rows,
+                               out=self._dev_resp)
+            self._pin_chi2.copy_(self._dev_chi2, non_blocking=True)
+            self._pin_resp.copy_(self._dev_resp, non_blocking=True)
 
     def results(self):
-        """Per patch (chi2[n_bands] f64, dchi2[n_bands, n_sources, 7] f32) from the last fetch."""
-        c = self._pin_chi2.numpy()
-        r = self._pin_resp.numpy()
-        out = []
-        for i, p in enumerate(self.patches):
-            out.append((c[i, :p.n_bands].copy(), response_view(r[i], p.n_bands, int(p.n_sources)).copy()))
-        return out
+        """Per patch (chi2[n_bands] f64, dchi2[n_bands, n_sources, 7] f32) from the
+        last fetch: views into one fresh copy of the fetched rows, so they stay
+        valid after later calls."""
+        c = self._pin_chi2.numpy().copy()
+        r = self._pin_resp.numpy().copy().reshape(-1, MAXSOURCES, NPARAMS)
+        return [(c[o:o + nb], r[o:o + nb, :ns]) for o, nb, ns in self._slices]
 
     # --- the public call ---
     def evaluate_proposals(self, proposals, stream=None):
@@ -154,7 +200,7 @@ class BatchedProposer:
 
     @property
     def d2h_bytes(self):
-        return int(self.plan.chi2.numel() * 8 + self.plan.response.numel() * 4)
+        return int(self._pin_chi2.numel() * 8 + self._pin_resp.numel() * 4)
 
     def count_pairs(self, stream=None):
         """(evaluated pairs, pairs within the cutoff, within-cutoff pairs culled) of one evaluation."""

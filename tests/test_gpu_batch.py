@@ -1,0 +1,98 @@
+"""The batched public call, ``BatchedProposer.evaluate_proposals``: parity of
+every patch of a mixed batch with the FP64 oracle and with the one-patch
+``B200Proposer`` (the same tiles, so the same sums), the staging of proposals
+of changing length, and results that stay valid after later calls."""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tolerances import CHI2_F64, GRAD_F64, chi2_err, chi2_scale, grad_err
+
+pytestmark = pytest.mark.gpu
+
+
+def _patches():
+    from forcepho_b200 import synthetic as S
+    shapes = [(3, 2, 1, 40), (7, 1, 2, 56), (2, 4, 1, 32), (12, 3, 2, 64), (5, 2, 1, 48)]
+    out = []
+    for i, (ns, nb, epb, size) in enumerate(shapes):
+        p = S.config_multiband(seed=300 + i, n_sources=ns, n_bands=nb, exp_per_band=epb, size=size)
+        p.return_residual = False
+        p.send_to_device()
+        out.append(p)
+    return out
+
+
+def _perturbed(patches, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for p in patches:
+        q = p.scene.get_proposal().copy()
+        q["ra"] += rng.normal(0, 2e-6, len(q)).astype(np.float32)
+        q["q"] = np.clip(q["q"] * rng.uniform(0.95, 1.05, len(q)), 0.2, 0.99).astype(np.float32)
+        out.append(q)
+    return out
+
+
+@pytest.fixture(scope="module")
+def batch():
+    return _patches()
+
+
+def test_batch_matches_oracle_and_single_patch(batch):
+    from forcepho_b200.batch import BatchedProposer
+    from forcepho_b200.proposal import B200Proposer
+    props = _perturbed(batch, 1)
+    bp = BatchedProposer(batch, tile_pixels=1024)
+    res = bp.evaluate_proposals(props)
+    single = B200Proposer(tile_pixels=1024)
+    for p, prop, (chi2, dchi2) in zip(batch, props, res):
+        assert chi2.shape == (p.n_bands,)
+        assert dchi2.shape == (p.n_bands, int(p.n_sources), 7)
+        c64, g64, r64 = O.evaluate(p, prop, precision="f64", return_residual=True)
+        scale = chi2_scale(chi2, p.data, p.ierr, r64)
+        assert chi2_err(chi2, c64, scale) < CHI2_F64
+        assert grad_err(dchi2, g64) < GRAD_F64
+        c1, g1 = single.evaluate_proposal(prop, patch=p)
+        np.testing.assert_array_equal(chi2, c1)
+        np.testing.assert_array_equal(dchi2, g1)
+
+
+def test_repeated_calls_and_result_lifetime(batch):
+    from forcepho_b200.batch import BatchedProposer
+    a, b = _perturbed(batch, 2), _perturbed(batch, 3)
+    bp = BatchedProposer(batch, tile_pixels=1024)
+    ra = bp.evaluate_proposals(a)
+    kept = [(c.copy(), g.copy()) for c, g in ra]
+    rb = bp.evaluate_proposals(b)
+    for (c, g), (c0, g0) in zip(ra, kept):          # earlier results are not overwritten
+        np.testing.assert_array_equal(c, c0)
+        np.testing.assert_array_equal(g, g0)
+    fresh = BatchedProposer(batch, tile_pixels=1024).evaluate_proposals(b)
+    for (c, g), (c2, g2) in zip(rb, fresh):
+        np.testing.assert_array_equal(c, c2)
+        np.testing.assert_array_equal(g, g2)
+
+
+def test_staging_zeroes_the_slots_of_a_shorter_proposal(batch):
+    from forcepho_b200.batch import BatchedProposer
+    from forcepho_b200.structs import source_struct_dtype
+    props = _perturbed(batch, 4)
+    bp = BatchedProposer(batch, tile_pixels=1024)
+    bp.set_proposals_async(props)
+    i = 3                                              # the 12-source patch
+    bp.set_proposals_async(props[:i] + [props[i][:5]] + props[i + 1:])
+    slots = bp._pin_prop.numpy().view(source_struct_dtype).reshape(len(batch), -1)
+    np.testing.assert_array_equal(slots[i, :5], props[i][:5])
+    assert not slots[i, 5:].view(np.uint8).any()
+    bp.set_proposals_async(props[:2])                  # patches past the list: no sources
+    assert not slots[2:].view(np.uint8).any()
+    with pytest.raises(ValueError):
+        bp.set_proposals_async(props + props[:1])
+    # and back to full proposals: results equal a fresh proposer's
+    res = bp.evaluate_proposals(props)
+    want = BatchedProposer(batch, tile_pixels=1024).evaluate_proposals(props)
+    for (c, g), (c2, g2) in zip(res, want):
+        np.testing.assert_array_equal(c, c2)
+        np.testing.assert_array_equal(g, g2)
