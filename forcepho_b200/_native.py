@@ -54,6 +54,7 @@ hmc_patch_dtype = np.dtype([("param_offset", np.int64), ("n_sources", np.int32),
 
 FLAG_NO_CULL = 1
 FLAG_STATIC = 2
+FLAG_FORWARD_ONLY = 4
 PHASE_SETUP, PHASE_TILES, PHASE_REDUCE = 1, 2, 4
 
 # return codes (include/forcepho_b200.h)

@@ -257,6 +257,7 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool nocull = (flags & FP_FLAG_NO_CULL) != 0;
+    const bool forward_only = (flags & FP_FLAG_FORWARD_ONLY) != 0;
 
     for (int64_t iter = 0;; ++iter) {
         if (tid == 0) {
@@ -442,7 +443,7 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
         for (int t = tid; t < FP_WARPS * MAXSOURCES * NPARAMS; t += FP_THREADS) s_wsrc[t] = 0.0;
 
         // ---- 3. adjoint: one Gaussian per lane, pixels broadcast ----
-        for (int c0 = 0; c0 < gc; c0 += FP_CHUNK) {
+        for (int c0 = 0; c0 < (forward_only ? 0 : gc); c0 += FP_CHUNK) {
             const int cn = min(FP_CHUNK, gc - c0);
             __syncthreads();
             if (gc > FP_CHUNK) {

@@ -149,6 +149,21 @@ class B200PatchMixin:
         self.device_ptrs = {}
         self.device_patch = None
 
+    # --- consumers of the kernel (device_patch.py:113-254), in forcepho_b200.render ---
+    def subtract_fixed(self, fixed, active=None, big=None, maxactive=15, swap_local=False,
+                       big_scene_kwargs=None, **scene_kwargs):
+        from .render import subtract_fixed
+        return subtract_fixed(self, fixed, active=active, big=big, maxactive=maxactive,
+                              swap_local=swap_local, big_scene_kwargs=big_scene_kwargs, **scene_kwargs)
+
+    def design_matrix(self, active=None, proposer=None, **scene_kwargs):
+        from .render import design_matrix
+        return design_matrix(self, active, proposer=proposer, **scene_kwargs)
+
+    def render(self, catalog, splinedata=None):
+        from .render import render
+        return render(self, catalog, splinedata=splinedata)
+
     # --- extras of this implementation ---
     @property
     def device_patch_ptr(self):

@@ -145,3 +145,8 @@ class PatchBase:
     def split_pix(self, attr):
         arr = getattr(self, attr)
         return np.split(arr, np.cumsum(self.exposure_N[:-1]))
+
+    def split_band(self, attr):
+        """A pixel array split by band (forcepho/patches/patch.py:610-620)."""
+        arr = getattr(self, attr)
+        return np.split(arr, np.cumsum(self.band_N_pix[:-1]))

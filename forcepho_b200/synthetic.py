@@ -49,13 +49,90 @@ __all__ = ["make_patch", "config_small", "config_multiband", "config_limits",
 
 
 class SyntheticPatch(B200PatchMixin, PatchBase):
-    """A PatchBase (with the device mixin) carrying the scene it was drawn from."""
+    """A PatchBase (with the device mixin) carrying the scene it was drawn from.
+
+    Like the reference's store-backed patches (forcepho/patches/patch.py:244-425)
+    it keeps what is needed to pack the source metadata of any scene over the
+    same pixels: each exposure's linear astrometry (``astrometry``: pixel =
+    cen_e + A_e arcsec-offset) and PSF block (``psf_blocks``), with
+    ``meta_for`` / ``pack_meta`` / ``set_scene``."""
 
     def __init__(self, **kw):
         super().__init__(**kw)
         self.scene = None
         self.sigma = None
         self.bandlist = None
+        self.astrometry = None
+        self.psf_blocks = None
+        self.splines = None
+
+    def meta_for(self, scene):
+        """The source-dependent metadata arrays of ``scene`` (its sources in
+        order) over this patch's exposures, without changing the patch:
+        ``n_sources, D, CW, crpix, crval, psfgauss, psfgauss_start``."""
+        A, cen = self.astrometry
+        srcs = list(scene.sources)
+        ns, ne = len(srcs), self.n_exp
+        dt = self.meta_dtype
+        D = np.zeros((ne, ns, 2, 2), dtype=dt)
+        CW = np.zeros((ne, ns, 2, 2), dtype=dt)
+        crpix = np.zeros((ne, ns, 2), dtype=dt)
+        crval = np.zeros((ne, ns, 2), dtype=dt)
+        for e in range(ne):
+            for s, g in enumerate(srcs):
+                cosd = np.cos(np.deg2rad(REF_COORD[1] + g.dec))
+                W = np.diag([cosd, 1.0])
+                D[e, s] = A[e]
+                CW[e, s] = 3600.0 * A[e] @ W
+                crval[e, s] = [g.ra, g.dec]
+                crpix[e, s] = cen[e] + A[e] @ (3600.0 * W @ np.array([g.ra, g.dec]))
+        # every source of an exposure gets a copy of the exposure's PSF block
+        blocks, pstart, k = [], [], 0
+        for e in range(ne):
+            one = self.psf_blocks[e]
+            pstart.append(k)
+            for _ in range(ns):
+                blocks.append(one)
+                k += len(one)
+        psfgauss = np.concatenate(blocks) if blocks else np.zeros(0, psf_dtype)
+        return dict(n_sources=ns, D=D, CW=CW, crpix=crpix, crval=crval, psfgauss=psfgauss,
+                    psfgauss_start=np.asarray(pstart, dtype=np.int32))
+
+    def pack_meta(self, scene):
+        """Make ``scene`` the patch's scene: repack its source metadata
+        (forcepho/patches/patch.py:244-272); pixels are untouched."""
+        for k, v in self.meta_for(scene).items():
+            setattr(self, k, v)
+        self.scene = scene
+
+    def set_scene(self, sourcecat, splinedata=None):
+        """A Scene of Galaxy sources from a structured catalog with fields
+        ``ra, dec, q, pa, sersic, rhalf`` (ra/dec as degree offsets from the
+        patch reference coordinate) and one flux field per name in
+        ``bandlist`` (forcepho/patches/patch.py:400-425)."""
+        splines = splinedata if splinedata is not None else self.splines
+        scene = Scene()
+        for row in np.atleast_1d(sourcecat):
+            g = Galaxy(filternames=self.bandlist, splines=splines)
+            g.flux[:] = [float(row[b]) for b in self.bandlist]
+            g.ra, g.dec = float(row["ra"]), float(row["dec"])
+            g.q, g.pa, g.sersic, g.rhalf = (float(row["q"]), float(row["pa"]), float(row["sersic"]),
+                                            float(row["rhalf"]))
+            scene.sources.append(g)
+        return scene
+
+    def catalog(self, scene=None):
+        """The structured catalog of a scene (default: the patch's), the inverse of ``set_scene``."""
+        scene = scene if scene is not None else self.scene
+        dt = np.dtype([(c, np.float64) for c in ("ra", "dec", "q", "pa", "sersic", "rhalf")] +
+                      [(b, np.float64) for b in self.bandlist])
+        cat = np.zeros(len(scene.sources), dtype=dt)
+        for i, g in enumerate(scene.sources):
+            cat[i]["ra"], cat[i]["dec"] = g.ra, g.dec
+            cat[i]["q"], cat[i]["pa"], cat[i]["sersic"], cat[i]["rhalf"] = g.q, g.pa, g.sersic, g.rhalf
+            for j, b in enumerate(self.bandlist):
+                cat[i][b] = g.flux[j]
+        return cat
 
 
 def _rot(t):
@@ -172,19 +249,11 @@ def make_patch(rng, *, n_sources, exp_per_band, exp_pix, n_psf, psf_anisotropic=
         g.q, g.pa, g.sersic, g.rhalf = sp["q"], sp["pa"], sp["sersic"], sp["rhalf"]
         scene.sources.append(g)
 
-    for e in range(n_exp):
-        for s, g in enumerate(scene.sources):
-            cosd = np.cos(np.deg2rad(REF_COORD[1] + g.dec))
-            W = np.diag([cosd, 1.0])
-            patch.D[e, s] = A[e]
-            patch.CW[e, s] = 3600.0 * A[e] @ W
-            patch.crval[e, s] = [g.ra, g.dec]
-            patch.crpix[e, s] = cen[e] + A[e] @ (3600.0 * W @ np.array([g.ra, g.dec]))
-
-    # --- PSFs: one mixture per band, replicated over radius bins and sources ---
+    # --- PSFs: one mixture per band, replicated over radius bins (and, in
+    # the packed metadata, over sources) ---
     psfs = [_psf_mixture(rng, n_psf, psf_anisotropic, psf_offsets) for _ in range(n_bands)]
     patch.n_psf_per_source[:] = n_radii * n_psf
-    blocks, pstart, k = [], [], 0
+    psf_blocks = []
     for e in range(n_exp):
         amps, pc, cov = psfs[band_of_exp[e]]
         one = np.zeros(n_radii * n_psf, dtype=psf_dtype)
@@ -192,16 +261,14 @@ def make_patch(rng, *, n_sources, exp_per_band, exp_pix, n_psf, psf_anisotropic=
             for i in range(n_psf):
                 j = r * n_psf + i
                 one[j] = (amps[i], pc[i, 0], pc[i, 1], cov[i, 0, 0], cov[i, 1, 1], cov[i, 0, 1], r)
-        pstart.append(k)
-        for s in range(n_sources):
-            blocks.append(one)
-            k += len(one)
-    patch.psfgauss = np.concatenate(blocks) if blocks else np.zeros(0, psf_dtype)
-    patch.psfgauss_start[:] = pstart
+        psf_blocks.append(one)
 
-    patch.scene = scene
+    patch.astrometry = (np.array(A), np.array(cen))
+    patch.psf_blocks = psf_blocks
+    patch.splines = splines
     patch.bandlist = bandlist
     patch.band_of_exp = band_of_exp
+    patch.pack_meta(scene)
     return patch
 
 

@@ -265,6 +265,8 @@ typedef struct fp_launch {
 
 #define FP_FLAG_NO_CULL     1   /* evaluate every (tile, Gaussian) pair (no bounding-box culling) */
 #define FP_FLAG_STATIC      2   /* static round-robin tile assignment instead of an atomic queue */
+#define FP_FLAG_FORWARD_ONLY 4  /* model, residual and chi2 only: the adjoint pass is skipped and the
+                                   Response records are zero (renders, fixed-source subtraction) */
 
 #define FP_PHASE_SETUP      1   /* image-Gaussian tables (must precede the tile phase) */
 #define FP_PHASE_TILES      2   /* the persistent tile kernel */
