@@ -2,7 +2,7 @@
 
 The reference samples one patch at a time with littlemcmc's NUTS
 (forcepho/fitting.py:254-411: ``run_lmc`` with ``get_pot``).  littlemcmc is a
-third-party package (littlemcmc 0.2, a standalone copy of PyMC3's NUTS) that is
+third-party package (littlemcmc == 0.2.0, pinned by the reference's requirements.txt; a standalone copy of PyMC3's NUTS) that is
 not installed here; this module restates its published algorithm:
 
 * multinomial NUTS (Betancourt 2017): trajectories grow by doubling in a
