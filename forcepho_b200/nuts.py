@@ -427,6 +427,7 @@ class BatchedNUTS:
             if not (is_tune and discard_tuned_samples):
                 trace.append(z.copy())
                 stats.append(st)
+        self.state = (z, lnp, g)            # where a further call to iterate() continues
         return np.array(trace).reshape(-1, self.s.P), stats
 
 
