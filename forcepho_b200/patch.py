@@ -135,7 +135,8 @@ class PatchBase:
         npsf = self.n_psf_per_source[eb].astype(np.int64)
         if np.any(npsf <= 0):
             raise ValueError("n_psf_per_source must be positive")
-        if np.any(self.psfgauss_start.astype(np.int64) + npsf > len(self.psfgauss)):
+        # with no sources the PSF blocks are never read (and are empty)
+        if n_s > 0 and np.any(self.psfgauss_start.astype(np.int64) + npsf > len(self.psfgauss)):
             raise ValueError("psfgauss_start + n_psf_per_source exceeds psfgauss")
         bins = self.psfgauss["sersic_bin"]
         if len(bins) and (bins.min() < 0 or bins.max() >= int(self.n_radii)):

@@ -66,3 +66,10 @@ def test_optimize_one_band_is_weighted_least_squares():
     want = np.linalg.lstsq((X * w).T, y * w, rcond=None)[0]
     np.testing.assert_allclose(flux[:, 0], want, rtol=1e-10)
     np.testing.assert_allclose(ATA, (X * w) @ (X * w).T, rtol=1e-12)
+
+
+def test_empty_scene_packs_and_validates():
+    p = _patch()
+    p.pack_meta(Scene([]))
+    assert p.n_sources == 0 and p.D.shape == (p.n_exp, 0, 2, 2) and len(p.psfgauss) == 0
+    assert p.validate()
