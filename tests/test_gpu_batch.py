@@ -1,7 +1,8 @@
 """The batched public call, ``BatchedProposer.evaluate_proposals``: parity of
 every patch of a mixed batch with the FP64 oracle and with the one-patch
 ``B200Proposer`` (the same tiles, so the same sums), the staging of proposals
-of changing length, and results that stay valid after later calls."""
+of changing length, results that stay valid after later calls, the pair
+census, and a plan over shuffled pixels without coordinates."""
 
 import numpy as np
 import pytest
@@ -96,3 +97,44 @@ def test_staging_zeroes_the_slots_of_a_shorter_proposal(batch):
     for (c, g), (c2, g2) in zip(res, want):
         np.testing.assert_array_equal(c, c2)
         np.testing.assert_array_equal(g, g2)
+
+
+def test_census_no_within_cutoff_pair_culled(batch):
+    from forcepho_b200.batch import BatchedProposer
+    bp = BatchedProposer(batch, tile_pixels=1024)
+    bp.set_proposals_async(_perturbed(batch, 5))
+    kept, active, dropped = bp.count_pairs()
+    assert dropped == 0
+    assert kept >= active > 0
+
+
+def test_shuffled_pixels_and_plan_without_coordinates():
+    """Pixels shuffled within their exposures and a plan without coordinates:
+    tiles are runs of the shuffled order with wide bounding boxes (little is
+    culled); results still match the oracle."""
+    import torch
+    from forcepho_b200 import synthetic as S
+    from forcepho_b200.device import Plan, pack_proposals, response_view
+
+    def render(p, prop):
+        return O.render(p, prop, precision="f64")
+    p = S.config_multiband(seed=60, render=render, n_sources=4, n_bands=2, exp_per_band=1, size=40)
+    rng = np.random.default_rng(1)
+    for e in range(p.n_exp):
+        s0, n = int(p.exposure_start[e]), int(p.exposure_N[e])
+        o = s0 + rng.permutation(n)
+        for name in ("xpix", "ypix", "data", "ierr"):
+            getattr(p, name)[s0:s0 + n] = getattr(p, name)[o]
+    p.return_residual = False
+    p.send_to_device()
+    prop = p.scene.get_proposal().copy()
+    prop["q"] *= 0.97
+    plan = Plan([p], tile_pixels=1024, compact_tiles=False)
+    plan.proposals.copy_(torch.from_numpy(pack_proposals([prop], 1).view(np.uint8).reshape(-1)))
+    plan.evaluate(plan.launch(ctas_per_sm=4))
+    chi2 = plan.chi2.cpu().numpy()[0, :p.n_bands]
+    dchi2 = response_view(plan.response.cpu().numpy()[0], p.n_bands, int(p.n_sources))
+    c64, g64, r64 = O.evaluate(p, prop, precision="f64", return_residual=True)
+    sc = chi2_scale(chi2, p.data, p.ierr, r64)
+    assert chi2_err(chi2, c64, sc) < CHI2_F64
+    assert grad_err(dchi2, g64) < GRAD_F64
