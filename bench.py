@@ -50,6 +50,22 @@ EX2_PER_PAIR = 2
 TILE_TRAFFIC = {("batched", 512, 1024): 6.00e9 + 220.83e6}
 
 
+def hbm_fraction(traffic_bytes, algorithmic_gbs, kernel_ms):
+    """DRAM bandwidth of the tile kernel against the measured HBM copy bandwidth
+    (MEASURED_PEAKS.json, else the 6650 GB/s fallback): from the ncu traffic of a
+    launch when known, and from the algorithmic pixel stream."""
+    peak, src = 6650.0, "fallback 6650 GB/s (no MEASURED_PEAKS.json)"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, src = float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs"
+    except (OSError, ValueError, KeyError):
+        pass
+    traffic_gbs = None if traffic_bytes is None else traffic_bytes / (kernel_ms * 1e-3) / 1e9
+    return {"peak_gbs": peak, "peak_source": src, "traffic_gbs": traffic_gbs,
+            "traffic_frac": None if traffic_gbs is None else traffic_gbs / peak,
+            "algorithmic_gbs": algorithmic_gbs, "algorithmic_frac": algorithmic_gbs / peak}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -450,6 +466,7 @@ def run_ours(args):
                 "ex2": {"achieved_per_s": EX2_PER_PAIR * active / (tile_ms * 1e-3), "peak_per_s": ex2_rate.value,
                         "frac": EX2_PER_PAIR * active / (tile_ms * 1e-3) / ex2_rate.value},
                 "hbm_gbs": 16.0 * sum(int(np.sum(p.exposure_N)) for p in patches) / (tile_ms * 1e-3) / 1e9}
+    roofline["hbm"] = hbm_fraction(roofline["traffic"], roofline["hbm_gbs"], tile_ms)
 
     # ---- end to end through the public API (host proposals in, results out) ----
     for _ in range(2):
