@@ -349,6 +349,12 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
             wy1 = fmaxf(wy1, __shfl_xor_sync(0xffffffffu, wy1, o));
         }
         if (nocull) { wx0 = wy0 = -INFINITY; wx1 = wy1 = INFINITY; }
+        // one row: every thread's pixels share their y (cell rows in row order),
+        // so the y-dependent products of a Gaussian are formed once per thread
+        bool same_y = true;
+#pragma unroll
+        for (int k = 1; k < P; ++k) same_y = same_y && (k >= nval || ys[k] == ys[0]);
+        const bool rowwise = __all_sync(0xffffffffu, same_y);
         double M[P];
 #pragma unroll
         for (int k = 0; k < P; ++k) M[k] = 0.0;
@@ -369,19 +375,39 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
                     float m[P];
 #pragma unroll
                     for (int k = 0; k < P; ++k) m[k] = 0.f;
-                    for (int i = r0; i < r1; ++i) {
-                        const float4 bx = s_gbox[i];
-                        if (bx.y < wx0 || bx.x > wx1 || bx.w < wy0 || bx.z > wy1) continue;
-                        const float4 A = s_ga[i], B = s_gb[i];
+                    if (rowwise) {
+                        for (int i = r0; i < r1; ++i) {
+                            const float4 bx = s_gbox[i];
+                            if (bx.y < wx0 || bx.x > wx1 || bx.w < wy0 || bx.z > wy1) continue;
+                            const float4 A = s_ga[i], B = s_gb[i];
+                            const float dy = ys[0] - A.y;
+                            const float ty = A.w * dy, uy = B.x * dy;     // c Fxy dy, c Fyy dy
 #pragma unroll
-                        for (int k = 0; k < P; ++k) {
-                            const float dx = xs[k] - A.x, dy = ys[k] - A.y;
-                            const float vx = fmaf(A.z, dx, A.w * dy);
-                            const float vy = fmaf(B.x, dy, A.w * dx);
-                            const float e = fmaf(dy, vy, dx * vx);
-                            const float g = fp_ex2(e);
-                            const float h = fmaf(B.z, fmaf(vx, vx, vy * vy), B.y);
-                            m[k] = (e < FP_CUT_SCALED) ? m[k] : fmaf(g, h, m[k]);
+                            for (int k = 0; k < P; ++k) {
+                                const float dx = xs[k] - A.x;
+                                const float vx = fmaf(A.z, dx, ty);
+                                const float vy = fmaf(A.w, dx, uy);
+                                const float e = fmaf(dy, vy, dx * vx);
+                                const float g = fp_ex2(e);
+                                const float h = fmaf(B.z, fmaf(vx, vx, vy * vy), B.y);
+                                m[k] = (e < FP_CUT_SCALED) ? m[k] : fmaf(g, h, m[k]);
+                            }
+                        }
+                    } else {
+                        for (int i = r0; i < r1; ++i) {
+                            const float4 bx = s_gbox[i];
+                            if (bx.y < wx0 || bx.x > wx1 || bx.w < wy0 || bx.z > wy1) continue;
+                            const float4 A = s_ga[i], B = s_gb[i];
+#pragma unroll
+                            for (int k = 0; k < P; ++k) {
+                                const float dx = xs[k] - A.x, dy = ys[k] - A.y;
+                                const float vx = fmaf(A.z, dx, A.w * dy);
+                                const float vy = fmaf(B.x, dy, A.w * dx);
+                                const float e = fmaf(dy, vy, dx * vx);
+                                const float g = fp_ex2(e);
+                                const float h = fmaf(B.z, fmaf(vx, vx, vy * vy), B.y);
+                                m[k] = (e < FP_CUT_SCALED) ? m[k] : fmaf(g, h, m[k]);
+                            }
                         }
                     }
 #pragma unroll
