@@ -32,6 +32,8 @@
 
 namespace {
 
+static_assert(FP_RUN == 32, "the forward pass sums runs of one 32-Gaussian ballot word");
+
 
 // ---------------------------------------------------------------------------
 // setup
@@ -369,16 +371,27 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
                 s_gbox[i] = gbox[gi];
             }
             __syncthreads();
-            if (nval > 0) {
-                for (int r0 = 0; r0 < cn; r0 += FP_RUN) {
-                    const int r1 = min(cn, r0 + FP_RUN);
+            {
+                // runs of 32 Gaussians: lane l tests Gaussian r0 + l against the
+                // warp's pixel box, and the warp visits the hits of the run in
+                // ascending order; each run is summed in FP32, then added in FP64.
+                // Every lane takes part in the ballot, including lanes without
+                // pixels (their sums are never used).
+                for (int r0 = 0; r0 < cn; r0 += 32) {
+                    const int il = r0 + lane;
+                    bool hit = false;
+                    if (il < cn) {
+                        const float4 bx = s_gbox[il];
+                        hit = !(bx.y < wx0 || bx.x > wx1 || bx.w < wy0 || bx.z > wy1);
+                    }
+                    unsigned word = __ballot_sync(0xffffffffu, hit);
                     float m[P];
 #pragma unroll
                     for (int k = 0; k < P; ++k) m[k] = 0.f;
                     if (rowwise) {
-                        for (int i = r0; i < r1; ++i) {
-                            const float4 bx = s_gbox[i];
-                            if (bx.y < wx0 || bx.x > wx1 || bx.w < wy0 || bx.z > wy1) continue;
+                        while (word) {
+                            const int i = r0 + __ffs(word) - 1;
+                            word &= word - 1u;
                             const float4 A = s_ga[i], B = s_gb[i];
                             const float dy = ys[0] - A.y;
                             const float ty = A.w * dy, uy = B.x * dy;     // c Fxy dy, c Fyy dy
@@ -394,9 +407,9 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
                             }
                         }
                     } else {
-                        for (int i = r0; i < r1; ++i) {
-                            const float4 bx = s_gbox[i];
-                            if (bx.y < wx0 || bx.x > wx1 || bx.w < wy0 || bx.z > wy1) continue;
+                        while (word) {
+                            const int i = r0 + __ffs(word) - 1;
+                            word &= word - 1u;
                             const float4 A = s_ga[i], B = s_gb[i];
 #pragma unroll
                             for (int k = 0; k < P; ++k) {
