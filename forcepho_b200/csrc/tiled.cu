@@ -212,7 +212,7 @@ __device__ __forceinline__ bool ellipse_meets_rect(const float4 A, float fys, fl
 }
 
 struct tile_smem {
-    size_t ga, gb, box, pix, wsrc, red, ints, idx, total;
+    size_t ga, gb, box, pix, wsrc, red, ints, keepw, idx, total;
 };
 
 __host__ __device__ inline tile_smem tile_smem_layout(int tile_pixels, int max_gauss)
@@ -226,6 +226,7 @@ __host__ __device__ inline tile_smem tile_smem_layout(int tile_pixels, int max_g
     L.wsrc = o; o += (size_t)FP_WARPS * MAXSOURCES * NPARAMS * 8;
     L.red = o;  o += 16 * 8;
     L.ints = o; o += 32 * 4;
+    L.keepw = o; o += (((size_t)max_gauss + 31) / 32 * 4 + 15) & ~(size_t)15;
     L.idx = o;  o += ((size_t)max_gauss * 2 + 15) & ~(size_t)15;
     L.total = o;
     return L;
@@ -256,6 +257,7 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
     double *s_red = reinterpret_cast<double *>(smem + L.red);
     int *s_int = reinterpret_cast<int *>(smem + L.ints);          // [0] item, [8..16) warp counts
     uint16_t *s_idx = reinterpret_cast<uint16_t *>(smem + L.idx);
+    unsigned *s_keepw = reinterpret_cast<unsigned *>(smem + L.keepw); // cull ballot words
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const bool nocull = (flags & FP_FLAG_NO_CULL) != 0;
@@ -287,10 +289,16 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
         }
 
         // ---- 1. cull (ascending-order compaction of surviving Gaussians) ----
+        // Each warp tests a contiguous share of the exposure's Gaussians, 32 at
+        // a time, and keeps the ballot words; after one barrier every warp
+        // writes its kept indices at its offset (the warps' shares ascend).
         const float bx0 = tl.bbox[0], bx1 = tl.bbox[1], by0 = tl.bbox[2], by1 = tl.bbox[3];
-        int gc = 0;
-        for (int g0 = 0; g0 < ng; g0 += FP_THREADS) {
-            const int g = g0 + tid;
+        const int nwords = (ng + 31) >> 5;
+        const int per_warp = (nwords + FP_WARPS - 1) / FP_WARPS;
+        const int wbeg = min(nwords, warp * per_warp), wend = min(nwords, wbeg + per_warp);
+        int mine = 0;
+        for (int wd = wbeg; wd < wend; ++wd) {
+            const int g = wd * 32 + lane;
             bool keep = false;
             if (g < ng) {
                 if (nocull) {
@@ -304,19 +312,24 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, keep);
-            if (lane == 0) s_int[8 + warp] = __popc(m);
-            __syncthreads();
-            int off = gc, tot = 0;
-#pragma unroll
-            for (int w = 0; w < FP_WARPS; ++w) {
-                const int cnt = s_int[8 + w];
-                off += (w < warp) ? cnt : 0;
-                tot += cnt;
-            }
-            if (keep) s_idx[off + __popc(m & ((1u << lane) - 1u))] = (uint16_t)g;
-            gc += tot;
-            __syncthreads();
+            if (lane == 0) s_keepw[wd] = m;
+            mine += __popc(m);
         }
+        if (lane == 0) s_int[8 + warp] = mine;
+        __syncthreads();
+        int gc = 0, koff = 0;
+#pragma unroll
+        for (int w = 0; w < FP_WARPS; ++w) {
+            const int cnt = s_int[8 + w];
+            koff += (w < warp) ? cnt : 0;
+            gc += cnt;
+        }
+        for (int wd = wbeg; wd < wend; ++wd) {
+            const unsigned m = s_keepw[wd];
+            if (m & (1u << lane)) s_idx[koff + __popc(m & ((1u << lane) - 1u))] = (uint16_t)(wd * 32 + lane);
+            koff += __popc(m);
+        }
+        __syncthreads();
 
         // ---- 2. forward: model of P pixels per thread ----
         // the tile's pixels are listed in the plan's pixel order (compact cells)
