@@ -7,20 +7,25 @@
 //                  the ex2 scale folded in, an FP32 bounding box of its
 //                  E = dx^T F dx <= MAX_EXP_ARG region, and the FP64 Jacobian.
 //   tile_kernel    persistent CTAs pop tiles (largest first).  Per tile:
-//                  1. cull: keep the Gaussians whose box meets the tile's pixel
-//                     box (every other Gaussian has E > MAX_EXP_ARG at every
-//                     pixel of the tile and contributes exactly nothing);
+//                  1. cull: keep the Gaussians whose box, and then whose
+//                     E <= MAX_EXP_ARG ellipse (FP64), meets the tile's pixel
+//                     box; every other Gaussian has E > MAX_EXP_ARG at every
+//                     pixel of the tile and contributes exactly nothing;
 //                  2. forward, pixel-parallel: P pixels per thread, Gaussians
-//                     streamed from shared memory, SFU ex2, FP32 runs of
-//                     FP_RUN Gaussians flushed into per-pixel FP64 sums;
-//                     residual, chi2 term in f64, w = r ierr^2;
+//                     staged in shared memory; per run of 32 Gaussians one box
+//                     test per lane and a warp ballot, the warp visiting only
+//                     the hits; y terms once per row of pixels; SFU ex2; FP32
+//                     runs flushed into per-pixel FP64 sums; residual, chi2
+//                     term in f64, w = r ierr^2;
 //                  3. adjoint, Gaussian-parallel: one Gaussian per lane, the
 //                     tile's nonzero-weight pixels broadcast from shared memory;
 //                     each lane accumulates 12 moments (FP32 runs -> FP64) from
 //                     which the 6 image-space partials follow exactly; the FP64
 //                     Jacobian maps them to the 7 on-sky partials once per
-//                     Gaussian, not once per pixel;
-//                  4. per-source sums in a fixed order -> per-tile partials.
+//                     (Gaussian, segment), not once per pixel;
+//                  4. per-source sums inside each warp (a segmented shuffle
+//                     tree), one fixed-order sum over the warps per tile ->
+//                     per-tile partials.
 //   reduce_kernel  per (patch, band): partials summed over the band's tiles in
 //                  canonical order (FP64) -> chi2 (f64) and Response (f32).
 // No atomics touch the results, so they are bitwise reproducible.
