@@ -1,0 +1,22 @@
+"""forcepho's likelihood hot path on B200 (sm_100a CUDA behind a C ABI).
+
+Modules, with the reference counterparts they stand in for:
+
+* ``proposal``    -- ``B200Proposer`` / ``PlainProposer`` (``forcepho.proposal.GPUProposer``)
+* ``device``      -- ``B200PatchMixin`` (``forcepho.patches.device_patch.GPUPatchMixin``) and
+                     ``Plan``, the device-resident work plan of many patches
+* ``batch``       -- ``BatchedProposer``: one proposal for each of many patches per launch
+* ``model``       -- ``FastPosterior``, ``BoundedTransform``, ``stack_grad`` (``forcepho.model``)
+* ``hmc``         -- ``DeviceHMC``: HMC of many patches with all state on the device
+* ``nuts``        -- ``BatchedNUTS``, ``run_nuts`` (``forcepho.fitting.run_lmc``)
+* ``render``      -- ``subtract_fixed``, ``design_matrix``, ``render`` (``device_patch.py``)
+* ``fitting``     -- ``optimize_one_band``, ``optimize_fluxes`` (``forcepho.fitting``)
+* ``autograd``    -- ``PatchChi2``, a ``torch.autograd.Function`` over the kernels
+* ``distributed`` -- ``PatchFarm``: patches shared out over processes / GPUs
+* ``sources``, ``patch``, ``structs``, ``kernel_limits``, ``splines`` -- the data
+  model (``forcepho.sources``, ``forcepho.patches.patch``, ``forcepho.kernel_limits``)
+* ``synthetic``   -- seeded synthetic patches of the benchmark workloads
+* ``build``, ``_native`` -- the in-tree CUDA library and its ctypes bindings
+
+Submodules are imported on use; importing the package itself loads nothing.
+"""
