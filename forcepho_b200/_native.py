@@ -76,6 +76,7 @@ SIGNATURES = {
     "fp_version": (ctypes.c_int, []),
     "fp_struct_sizes": (ctypes.c_int, [c_vp]),
     "fp_evaluate_proposal_plain": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp]),
+    "fp_evaluate_proposal": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp]),
     "fp_plan_count": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PlanSizes)]),
     "fp_plan_fill": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "fp_plan_bbox": (ctypes.c_int, [c_vp, ctypes.POINTER(PlanSizes), ctypes.POINTER(PlanTables), c_vp]),

@@ -16,7 +16,8 @@
  *   - Entry points never allocate device memory: buffers are owned by the caller
  *     (the reference's Python patch objects own theirs, forcepho/patches/device_patch.py:265-297).
  *   - Launches are asynchronous on `stream` and contain no host synchronisation, so a
- *     sequence of them can be captured into a CUDA graph.
+ *     sequence of them can be captured into a CUDA graph.  The one exception is
+ *     fp_evaluate_proposal, which reads the patch struct back before its launch.
  */
 #ifndef FORCEPHO_B200_H
 #define FORCEPHO_B200_H
@@ -152,6 +153,17 @@ FP_API int fp_struct_sizes(int32_t out[4]);
 FP_API int fp_evaluate_proposal_plain(const fp_patch *d_patch, const fp_source *d_proposal,
                                int n_bands, int max_gauss_per_exposure,
                                double *d_chi2, fp_response *d_response, void *stream);
+
+/* The same evaluation with the kernel ABI of the reference's
+ * EvaluateProposal (forcepho/src/compute_gaussians_kernel.cu:212-214): device
+ * patch, device sources, output chi2[n_bands] and Response[n_bands].  It sizes
+ * shared memory from the patch itself, so it copies the 152-byte struct and
+ * n_psf_per_source[n_bands] back to the host and waits for them on `stream`
+ * before the launch (the result is still produced asynchronously on
+ * `stream`).  n_sources must equal the struct's n_sources (FP_ERR_ARGUMENT
+ * otherwise).  For many patches, or the tiled kernels, use fp_evaluate_batch. */
+FP_API int fp_evaluate_proposal(const fp_patch *d_patch, const fp_source *d_sources, int n_sources,
+                                int n_bands, double *d_chi2, fp_response *d_response, void *stream);
 
 /* ------------------------------------------------------------------------- */
 /* Tiled / batched path.                                                     */
