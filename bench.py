@@ -362,7 +362,9 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        # ranks that wait for each other end with an error within 5 minutes; rank 0's
+        # CPU legs (about a minute) run while the others wait at the last barrier
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     else:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
