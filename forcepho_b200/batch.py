@@ -79,7 +79,9 @@ class BatchedProposer:
         self._pin_chi2 = torch.zeros(len(rows), dtype=torch.float64).pin_memory()
         self._pin_resp = torch.zeros((len(rows), MAXSOURCES * NPARAMS), dtype=torch.float32).pin_memory()
         offsets = np.concatenate([[0], np.cumsum(nb)[:-1]]).astype(int)
-        self._slices = [(int(o), nb[i], int(self.patches[i].n_sources)) for i, o in enumerate(offsets)]
+        self._slices = [(slice(int(o), int(o) + nb[i]), (slice(int(o), int(o) + nb[i]),
+                                                         slice(0, int(self.patches[i].n_sources))))
+                        for i, o in enumerate(offsets)]
 
     # --- launch parameters ---
     def _autotune(self, tuner):
@@ -121,10 +123,10 @@ class BatchedProposer:
         slots, lens = self._prop_slots, self._prop_len
         for i in range(self.n):
             if i < len(proposals):
-                p = np.asarray(proposals[i])
-                if p.dtype != source_struct_dtype:
-                    p = p.astype(source_struct_dtype)
-                p = np.ascontiguousarray(p).reshape(-1)
+                p = proposals[i]
+                if not (type(p) is np.ndarray and p.dtype == source_struct_dtype and p.ndim == 1
+                        and p.flags.c_contiguous):
+                    p = np.ascontiguousarray(np.asarray(p).astype(source_struct_dtype, copy=False)).reshape(-1)
                 k = len(p)
                 if k > MAXSOURCES:
                     raise ValueError("proposal %d has %d sources > MAXSOURCES=%d" % (i, k, MAXSOURCES))
@@ -178,7 +180,7 @@ class BatchedProposer:
         valid after later calls."""
         c = self._pin_chi2.numpy().copy()
         r = self._pin_resp.numpy().copy().reshape(-1, MAXSOURCES, NPARAMS)
-        return [(c[o:o + nb], r[o:o + nb, :ns]) for o, nb, ns in self._slices]
+        return [(c[a], r[b]) for a, b in self._slices]
 
     # --- the public call ---
     def evaluate_proposals(self, proposals, stream=None):
