@@ -19,7 +19,7 @@ from scipy.special import expit
 
 from .kernel_limits import NPARAMS
 
-__all__ = ["Posterior", "FastPosterior", "Transform", "BoundedTransform", "stack_grad",
+__all__ = ["Posterior", "FastPosterior", "GPUPosterior", "Transform", "BoundedTransform", "stack_grad",
            "sigmoid", "logit", "sigmoid_grad"]
 
 
@@ -165,6 +165,11 @@ class FastPosterior(Posterior):
         self.patch.return_residual = orig
         self._residuals = ret[2]
         return self._residuals
+
+
+class GPUPosterior(FastPosterior):
+    """The reference's backwards-compatible name for ``FastPosterior``
+    (forcepho/model.py:408-411)."""
 
 
 def sigmoid(x):
