@@ -592,10 +592,12 @@ def run_hmc(args):
     props_dev = torch.cuda.get_device_properties(0)
     gpu_id = ("GPU-" + str(props_dev.uuid)) if getattr(props_dev, "uuid", None) else "0"
     with ClockSampler(gpu_id) as clk:
+        torch.cuda.nvtx.range_push("bench_timed")
         e0.record(stream)
         h.run(args.steps)
         e1.record(stream)
         e1.synchronize()
+        torch.cuda.nvtx.range_pop()
     ms = e0.elapsed_time(e1)
     grad_evals = n * args.hmc_steps * args.steps
     pairs = h.plan.n_pairs * args.hmc_steps * args.steps
