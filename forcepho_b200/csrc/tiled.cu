@@ -18,7 +18,10 @@
 //                     runs flushed into per-pixel FP64 sums; residual, chi2
 //                     term in f64, w = r ierr^2;
 //                  3. adjoint, Gaussian-parallel: one Gaussian per lane, the
-//                     tile's nonzero-weight pixels broadcast from shared memory;
+//                     tile's nonzero-weight pixels broadcast from shared memory
+//                     (a chunk's last, partial group of v Gaussians is
+//                     replicated over the idle lanes, each replica taking every
+//                     k-th pixel, and the replicas summed by shuffles);
 //                     each lane accumulates 12 moments (FP32 runs -> FP64) from
 //                     which the 6 image-space partials follow exactly; the FP64
 //                     Jacobian maps them to the 7 on-sky partials once per
@@ -38,6 +41,11 @@
 namespace {
 
 static_assert(FP_RUN == 32, "the forward pass sums runs of one 32-Gaussian ballot word");
+
+// A chunk's last group of v < 32 Gaussians is replicated min(8, 32 / v) times
+// across the warp's lanes in the adjoint, each replica taking every k-th pixel;
+// 8 replicas read 8 consecutive float4 (128 B) per step.
+constexpr int FP_MAX_REPLICAS = 8;
 
 
 // ---------------------------------------------------------------------------
@@ -122,23 +130,25 @@ __global__ void bbox_kernel(const fp_patch *const *__restrict__ patches,
 // ---------------------------------------------------------------------------
 // tile kernel helpers
 // ---------------------------------------------------------------------------
-// Adjoint moments of one Gaussian (params A, B) over pixels [p0, p1) of the
-// tile's nonzero-weight list.  With K = w' 2^(cE) (w' = -2 r ierr^2, zero past
+// Adjoint moments of one Gaussian (params A, B) over pixels p0, p0 + k, ... < p1
+// of the tile's nonzero-weight list (k = 1 unless STRIDED).  With K = w' 2^(cE) (w' = -2 r ierr^2, zero past
 // the cutoff), H the pixel-integral factor and v' = c F dx:
 //   m0 K, m1 KH, m2 KH vx', m3 KH vy', m4 K vx', m5 K vy', m6 KH dx^2,
 //   m7 KH dy^2, m8 KH dx dy, m9 K dx vx', m10 K dy vy', m11 K (dx vy' + dy vx')
+template <bool STRIDED>
 __device__ __forceinline__ void adjoint_moments(const float4 A, const float4 B,
-                                                const float4 *__restrict__ s_pix, int p0, int p1,
+                                                const float4 *__restrict__ s_pix, int p0, int p1, int k,
                                                 double (&m)[12])
 {
     const float xc = A.x, yc = A.y, fxs = A.z, fxys = A.w, fys = B.x, k0 = B.w;
     const float c24 = (float)FP_C24;
-    for (int r0 = p0; r0 < p1; r0 += FP_RUN) {
-        const int r1 = min(p1, r0 + FP_RUN);
+    const int step = STRIDED ? k : 1;
+    for (int r0 = p0; r0 < p1; r0 += FP_RUN * step) {
+        const int r1 = min(p1, r0 + FP_RUN * step);
         float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, a4 = 0.f, a5 = 0.f;
         float a6 = 0.f, a7 = 0.f, a8 = 0.f, a9 = 0.f, a10 = 0.f, a11 = 0.f;
 #pragma unroll 4
-        for (int p = r0; p < r1; ++p) {
+        for (int p = r0; p < r1; p += step) {
             const float4 q = s_pix[p];
             const float dx = q.x - xc, dy = q.y - yc;
             const float vx = fmaf(fxs, dx, fxys * dy);
@@ -513,24 +523,56 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
             // the (group of 32 Gaussians) x (pixel) plane, split evenly over the warps
             __syncthreads();
             const int ngrp = (cn + 31) >> 5;
-            const int64_t W = (int64_t)ngrp * nzt;
-            int64_t u = W * warp / FP_WARPS;
-            const int64_t u1 = W * (warp + 1) / FP_WARPS;
+            const int vlast = cn - ((ngrp - 1) << 5);             // Gaussians in the last group
+            const int krep = min(FP_MAX_REPLICAS, 32 / vlast);   // its replicas
+            const int ulast = (nzt + krep - 1) / krep;            // its units of krep pixels
+            // units of the (group, pixel) plane: at most 8 groups x 1024 pixels
+            const int ufull = (ngrp - 1) * nzt;
+            const int W = ufull + ulast;
+            int u = W * warp / FP_WARPS;
+            const int u1 = W * (warp + 1) / FP_WARPS;
             while (u < u1) {
-                const int grp = (int)(u / nzt);
-                const int p0 = (int)(u - (int64_t)grp * nzt);
-                const int p1 = (int)min((int64_t)nzt, (int64_t)p0 + (u1 - u));
-                const int gl = grp * 32 + lane;
-                const bool valid = gl < cn;
+                int grp, q0, qn;
+                if (u < ufull) {
+                    grp = u / nzt;
+                    q0 = u - grp * nzt;
+                    qn = nzt;
+                } else {
+                    grp = ngrp - 1;
+                    q0 = u - ufull;
+                    qn = ulast;
+                }
+                const int q1 = min(qn, q0 + (u1 - u));
+                const int kr = (grp == ngrp - 1) ? krep : 1;      // warp-uniform
+                const int vg = (grp == ngrp - 1) ? vlast : 32;
+                const int rep = lane / vg;
+                const int gl = grp * 32 + lane - rep * vg;
+                const bool valid = rep < kr && gl < cn;
                 const float4 A = valid ? s_ga[gl] : make_float4(0.f, 0.f, 0.f, 0.f);
                 const float4 B = valid ? s_gb[gl] : make_float4(0.f, 0.f, 0.f, 0.f);
                 double mom[12];
 #pragma unroll
                 for (int k = 0; k < 12; ++k) mom[k] = 0.0;
-                adjoint_moments(A, B, s_pix, p0, p1, mom);
+                if (kr == 1) {
+                    adjoint_moments<false>(A, B, s_pix, q0, q1, 1, mom);
+                } else {
+                    // replica rep takes pixels q*kr + rep of units [q0, q1): the
+                    // warp reads kr consecutive pixels per step
+                    const int pe = min(nzt, q1 * kr);
+                    adjoint_moments<true>(A, B, s_pix, valid ? q0 * kr + rep : pe, pe, kr, mom);
+                    // sum the replicas into replica 0 (lanes 0 .. vg-1), fixed tree
+                    for (int o = 1; o < kr; o <<= 1) {
+                        const bool take = (rep & (2 * o - 1)) == 0 && rep + o < kr;
+#pragma unroll
+                        for (int k = 0; k < 12; ++k) {
+                            const double t = __shfl_down_sync(0xffffffffu, mom[k], o * vg);
+                            if (take) mom[k] += t;
+                        }
+                    }
+                }
                 double g7[NPARAMS];
                 int src = -1;
-                if (valid) {
+                if (valid && rep == 0) {
                     const int gidx = s_idx[c0 + gl];
                     moments_to_grad(gjac + (size_t)FP_JAC * (ed.gauss_offset + gidx), mom, g7);
                     src = gidx / n_psf;               // Gaussian g belongs to source g / n_psf
@@ -552,13 +594,13 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
                     }
                 }
                 const int sprev = __shfl_up_sync(0xffffffffu, src, 1);
-                if (valid && (lane == 0 || sprev != src)) {
+                if (src >= 0 && (lane == 0 || sprev != src)) {
                     double *row = s_wsrc + ((size_t)warp * MAXSOURCES + src) * NPARAMS;
 #pragma unroll
                     for (int k = 0; k < NPARAMS; ++k) row[k] += g7[k];
                 }
                 __syncwarp();   // another lane may update the same row in the next segment
-                u += p1 - p0;
+                u += q1 - q0;
             }
         }
         __syncthreads();
