@@ -183,8 +183,11 @@ extern "C" int fp_evaluate_proposal_plain(const fp_patch *d_patch, const fp_sour
                             "fp_evaluate_proposal_plain: %d image Gaussians per exposure need %zu B "
                             "of shared memory (device limit %d B)",
                             max_gauss_per_exposure, smem, optin);
+    // the device's limit rather than this call's size: the attribute is per
+    // function, and a smaller value set by a concurrent call must not undercut
+    // a larger launch
     if (int rc = fp_check_cuda(cudaFuncSetAttribute(plain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    (int)smem),
+                                                    optin),
                                "cudaFuncSetAttribute(plain_kernel)"))
         return rc;
     plain_kernel<<<n_bands, PLAIN_THREADS, smem, (cudaStream_t)stream>>>(d_patch, d_proposal, d_chi2,

@@ -699,7 +699,11 @@ count_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc
     }
 }
 
-bool g_attr_set[8][3];
+// Whether tile_kernel<P> (index 0, 1, 2 for P = 1, 2, 4) has had its dynamic
+// shared-memory limit raised on a device.  Devices past the table set it on
+// every launch (the call is idempotent).
+constexpr int ATTR_MAX_DEVICES = 64;
+std::atomic<bool> g_attr_set[ATTR_MAX_DEVICES][3];
 
 template <int P>
 int launch_tiles(int grid, size_t smem, cudaStream_t st, const fp_patch *const *d_patches,
@@ -709,7 +713,7 @@ int launch_tiles(int grid, size_t smem, cudaStream_t st, const fp_patch *const *
     int dev = 0;
     if (int rc = fp_check_cuda(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
     const int pi = P == 1 ? 0 : (P == 2 ? 1 : 2);
-    if (dev < 8 && !g_attr_set[dev][pi]) {
+    if (dev < 0 || dev >= ATTR_MAX_DEVICES || !g_attr_set[dev][pi].load()) {
         int optin = 0;
         if (int rc = fp_check_cuda(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev),
                                    "cudaDeviceGetAttribute"))
@@ -718,7 +722,7 @@ int launch_tiles(int grid, size_t smem, cudaStream_t st, const fp_patch *const *
                                                         optin),
                                    "cudaFuncSetAttribute(tile_kernel)"))
             return rc;
-        g_attr_set[dev][pi] = true;
+        if (dev >= 0 && dev < ATTR_MAX_DEVICES) g_attr_set[dev][pi].store(true);
     }
     tile_kernel<P><<<grid, FP_THREADS, smem, st>>>(d_patches, tb.expos, tb.tiles, tb.order, tb.perm, n_tiles,
                                                     gfwd, gbox, gjac, partials, ctl, max_gauss, flags);
