@@ -82,6 +82,11 @@ class BatchedProposer:
         self._slices = [(slice(int(o), int(o) + nb[i]), (slice(int(o), int(o) + nb[i]),
                                                          slice(0, int(self.patches[i].n_sources))))
                         for i, o in enumerate(offsets)]
+        # completion of the last copy out of the proposal staging buffer and of
+        # the last copy into the result buffers: the host waits on them before
+        # rewriting the one or reading the others
+        self._h2d_done = None
+        self._d2h_done = None
 
     # --- launch parameters ---
     def _autotune(self, tuner):
@@ -120,6 +125,8 @@ class BatchedProposer:
         their copy to the device."""
         if len(proposals) > self.n:
             raise ValueError("%d proposals for %d patches" % (len(proposals), self.n))
+        if self._h2d_done is not None:
+            self._h2d_done.synchronize()     # the previous copy may still read the buffer
         slots, lens = self._prop_slots, self._prop_len
         for i in range(self.n):
             if i < len(proposals):
@@ -139,6 +146,8 @@ class BatchedProposer:
         s = stream or torch.cuda.current_stream()
         with torch.cuda.stream(s):
             self.plan.proposals.copy_(self._pin_prop, non_blocking=True)
+        self._h2d_done = torch.cuda.Event()
+        self._h2d_done.record(s)
 
     def run(self, stream=None):
         """Queue one evaluation of the device proposals (graph replay when captured)."""
@@ -173,11 +182,15 @@ class BatchedProposer:
                                out=self._dev_resp)
             self._pin_chi2.copy_(self._dev_chi2, non_blocking=True)
             self._pin_resp.copy_(self._dev_resp, non_blocking=True)
+        self._d2h_done = torch.cuda.Event()
+        self._d2h_done.record(s)
 
     def results(self):
         """Per patch (chi2[n_bands] f64, dchi2[n_bands, n_sources, 7] f32) from the
-        last fetch: views into one fresh copy of the fetched rows, so they stay
-        valid after later calls."""
+        last fetch (waiting for its copies to land): views into one fresh copy
+        of the fetched rows, so they stay valid after later calls."""
+        if self._d2h_done is not None:
+            self._d2h_done.synchronize()
         c = self._pin_chi2.numpy().copy()
         r = self._pin_resp.numpy().copy().reshape(-1, MAXSOURCES, NPARAMS)
         return [(c[a], r[b]) for a, b in self._slices]

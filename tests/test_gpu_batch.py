@@ -1,8 +1,9 @@
 """The batched public call, ``BatchedProposer.evaluate_proposals``: parity of
 every patch of a mixed batch with the FP64 oracle and with the one-patch
 ``B200Proposer`` (the same tiles, so the same sums), the staging of proposals
-of changing length, results that stay valid after later calls, the pair
-census, and a plan over shuffled pixels without coordinates."""
+of changing length, results that stay valid after later calls, the
+asynchronous calls without a host synchronisation, the pair census, and a plan
+over shuffled pixels without coordinates."""
 
 import numpy as np
 import pytest
@@ -97,6 +98,29 @@ def test_staging_zeroes_the_slots_of_a_shorter_proposal(batch):
     for (c, g), (c2, g2) in zip(res, want):
         np.testing.assert_array_equal(c, c2)
         np.testing.assert_array_equal(g, g2)
+
+
+def test_async_calls_without_host_sync(batch):
+    """set_proposals_async / run / fetch_async / results with no synchronisation
+    by the caller: restaging waits only for the previous copy out of the
+    staging buffer, and results() waits for its own fetch."""
+    from forcepho_b200.batch import BatchedProposer
+    a, b = _perturbed(batch, 6), _perturbed(batch, 7)
+    ref = BatchedProposer(batch, tile_pixels=1024)
+    want_a, want_b = ref.evaluate_proposals(a), ref.evaluate_proposals(b)
+    bp = BatchedProposer(batch, tile_pixels=1024)
+    bp.set_proposals_async(a)
+    bp.run()
+    bp.fetch_async()
+    bp.set_proposals_async(b)
+    got_a = bp.results()
+    bp.run()
+    bp.fetch_async()
+    got_b = bp.results()
+    for got, want in ((got_a, want_a), (got_b, want_b)):
+        for (c, g), (c2, g2) in zip(got, want):
+            np.testing.assert_array_equal(c, c2)
+            np.testing.assert_array_equal(g, g2)
 
 
 def test_census_no_within_cutoff_pair_culled(batch):
