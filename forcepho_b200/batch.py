@@ -125,6 +125,7 @@ class BatchedProposer:
         their copy to the device."""
         if len(proposals) > self.n:
             raise ValueError("%d proposals for %d patches" % (len(proposals), self.n))
+        self.plan.check_current()            # a captured graph replays the plan's tables
         if self._h2d_done is not None:
             self._h2d_done.synchronize()     # the previous copy may still read the buffer
         slots, lens = self._prop_slots, self._prop_len

@@ -27,6 +27,7 @@ device patches, their bounding boxes, the workspace and the output buffers.
 """
 
 import ctypes
+import itertools
 
 import numpy as np
 import torch
@@ -54,6 +55,11 @@ def to_device_bytes(arr, device):
 
 def _ptr(t):
     return int(t.data_ptr())
+
+
+# numbers each upload of a patch (``send_to_device``): a re-sent patch may get
+# the same device addresses back from the allocator with other pixels in them
+_UPLOADS = itertools.count(1)
 
 
 class _DeviceArray:
@@ -103,6 +109,7 @@ class B200PatchMixin:
             self._alloc_residual()
         self.send_patchstruct_to_device()
         self._dirty_data = False
+        self.device_generation = next(_UPLOADS)
         return self.device_patch
 
     def _alloc_residual(self):
@@ -148,6 +155,7 @@ class B200PatchMixin:
     def free(self):
         self.device_ptrs = {}
         self.device_patch = None
+        self.device_generation = None
 
     # --- consumers of the kernel (device_patch.py:113-254), in forcepho_b200.render ---
     def subtract_fixed(self, fixed, active=None, big=None, maxactive=15, swap_local=False,
@@ -170,9 +178,11 @@ class B200PatchMixin:
         return _ptr(self.device_patch)
 
     def plan_signature(self):
-        """What a work plan depends on: the pixel layout and the scene's shape."""
+        """What a work plan depends on: the upload, the pixel layout and the
+        scene's shape."""
         d = self.device_ptrs
-        return (int(self.n_sources), self.npix, d["xpix"].ptr, d["ypix"].ptr,
+        return (getattr(self, "device_generation", None), int(self.n_sources), self.npix, d["xpix"].ptr,
+                d["ypix"].ptr,
                 tuple(np.asarray(self.exposure_start).tolist()), tuple(np.asarray(self.exposure_N).tolist()),
                 tuple(np.asarray(self.band_N).tolist()), tuple(np.asarray(self.n_psf_per_source).tolist()))
 
@@ -216,6 +226,9 @@ class Plan:
         self.tables = N.PlanTables(_ptr(self.d_expos), _ptr(self.d_tiles), _ptr(self.d_order),
                                    _ptr(self.d_bands), _ptr(self.d_perm))
         self.d_patches = torch.zeros(self.n, dtype=torch.int64, device=dev)
+        # what the tables were made from: each patch's upload and device struct
+        # (holding the struct keeps its memory from being reused)
+        self._stamps = [(getattr(p, "device_generation", None), p.device_patch) for p in self.patches]
         self.refresh_patch_pointers()
         st = current_stream_ptr(stream)
         N.check(self.L.fp_plan_bbox(_ptr(self.d_patches), ctypes.byref(sz), ctypes.byref(self.tables), st),
@@ -225,6 +238,14 @@ class Plan:
                                      device=dev)
         self.chi2 = torch.zeros((self.n, MAXBANDS), dtype=torch.float64, device=dev)
         self.response = torch.zeros((self.n, MAXBANDS, MAXSOURCES * NPARAMS), dtype=torch.float32, device=dev)
+
+    def check_current(self):
+        """Raise if a patch was freed or sent to the device again since the plan
+        was made: its tiles, pixel order and boxes describe the old upload."""
+        for i, (p, (gen, struct)) in enumerate(zip(self.patches, self._stamps)):
+            if getattr(p, "device_generation", None) != gen or getattr(p, "device_patch", None) is not struct:
+                raise RuntimeError("patch %d was freed or sent to the device again after this plan was made; "
+                                   "make a new plan (or proposer) for it" % i)
 
     def refresh_patch_pointers(self):
         ptrs = torch.tensor([p.device_patch_ptr for p in self.patches], dtype=torch.int64)
@@ -250,6 +271,7 @@ class Plan:
         """Queue one evaluation of the proposals in ``self.proposals`` (or the
         given device buffer) on ``stream``; outputs land in ``self.chi2`` /
         ``self.response`` (or the given buffers).  No host synchronisation."""
+        self.check_current()
         lp = launch if launch is not None else self.launch()
         props = self.proposals if proposals is None else proposals
         c2 = self.chi2 if chi2 is None else chi2

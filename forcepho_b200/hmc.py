@@ -183,6 +183,7 @@ class DeviceHMC:
     def run(self, n_traj, adapt=False, target=0.65):
         """Run n_traj trajectories (graph replays).  With ``adapt`` the step
         size of each patch follows the acceptance of each trajectory."""
+        self.plan.check_current()
         if self.graph is None:
             self.capture()
         if int(self.traj.item()) + n_traj > self.max_traj:

@@ -2,8 +2,9 @@
 every patch of a mixed batch with the FP64 oracle and with the one-patch
 ``B200Proposer`` (the same tiles, so the same sums), the staging of proposals
 of changing length, results that stay valid after later calls, the
-asynchronous calls without a host synchronisation, the pair census, and a plan
-over shuffled pixels without coordinates."""
+asynchronous calls without a host synchronisation, re-planning after a patch
+is sent again, the pair census, and a plan over shuffled pixels without
+coordinates."""
 
 import numpy as np
 import pytest
@@ -121,6 +122,34 @@ def test_async_calls_without_host_sync(batch):
         for (c, g), (c2, g2) in zip(got, want):
             np.testing.assert_array_equal(c, c2)
             np.testing.assert_array_equal(g, g2)
+
+
+def test_patch_sent_again_gets_a_new_plan():
+    """A proposer kept across uploads of one patch object re-plans for the new
+    pixels (here the same shapes, coordinates shifted by 7 px, which the
+    allocator may place at the old addresses); plans and batched proposers
+    made before the upload refuse to run."""
+    from forcepho_b200 import synthetic as S
+    from forcepho_b200.batch import BatchedProposer
+    from forcepho_b200.proposal import B200Proposer
+    p = S.config_multiband(seed=310, n_sources=3, n_bands=2, exp_per_band=1, size=40)
+    p.return_residual = False
+    p.send_to_device()
+    prop = p.scene.get_proposal()
+    pr = B200Proposer()
+    pr.evaluate_proposal(prop, patch=p)
+    old_plan = pr._plan
+    bp = BatchedProposer([p], tile_pixels=1024)
+    p.xpix = (p.xpix + 7).astype(p.xpix.dtype)
+    p.send_to_device()
+    c, g = pr.evaluate_proposal(prop, patch=p)
+    c2, g2 = B200Proposer().evaluate_proposal(prop, patch=p)
+    np.testing.assert_array_equal(c, c2)
+    np.testing.assert_array_equal(g, g2)
+    with pytest.raises(RuntimeError):
+        old_plan.evaluate()
+    with pytest.raises(RuntimeError):
+        bp.evaluate_proposals([prop])
 
 
 def test_census_no_within_cutoff_pair_culled(batch):
