@@ -43,18 +43,28 @@ def spline_table(device, splines=None):
     return tab
 
 
+def source_cos_dec(patch, n_sources):
+    """cos(dec) at each source, from the patch's own astrometry of its first
+    exposure: CW (pixels per degree) = 3600 D (pixels per arcsec) diag(cos dec, 1)."""
+    D = np.asarray(patch.D, np.float64)[0, :n_sources]
+    CW = np.asarray(patch.CW, np.float64)[0, :n_sources]
+    c = np.linalg.solve(D, CW)[:, 0, 0] / 3600.0
+    return np.where(np.isfinite(c) & (c > 0), c, 1.0)
+
+
 def default_bounds(patch, theta0):
     """Sampling bounds around a starting point, per parameter of ``theta0``
-    (one patch): flux in (0, 3 f0 + 1], positions within 0.3 arcsec, q in
-    [0.2, 1], pa in [-2, 2] rad, sersic in the spline table's range, rhalf in
-    [0.03, 0.6] arcsec."""
+    (one patch): flux in (0, 3 f0 + 1], positions within 0.3 arcsec (in RA
+    degrees scaled by 1 / cos dec at each source), q in [0.2, 1], pa in
+    [-2, 2] rad, sersic in the spline table's range, rhalf in [0.03, 0.6]
+    arcsec."""
     nb = patch.n_bands
     nper = nb + NPARAMS - 1
     th = np.asarray(theta0, np.float64).reshape(-1, nper)
     lo, hi = np.zeros_like(th), np.zeros_like(th)
     lo[:, :nb] = 0.0
     hi[:, :nb] = 3.0 * np.abs(th[:, :nb]) + 1.0
-    cosd = np.cos(np.deg2rad(-27.8))
+    cosd = source_cos_dec(patch, len(th))
     dpos = 0.3 / 3600.0
     lo[:, nb], hi[:, nb] = th[:, nb] - dpos / cosd, th[:, nb] + dpos / cosd
     lo[:, nb + 1], hi[:, nb + 1] = th[:, nb + 1] - dpos, th[:, nb + 1] + dpos
