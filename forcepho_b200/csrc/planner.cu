@@ -110,10 +110,13 @@ void exposure_tiles(const fp_patch_shape &s, int e, int tile_pixels, std::vector
             y0 = std::min(y0, yi); y1 = std::max(y1, yi);
         }
     }
+    // at most 2^30 cells per axis, so cell keys fit in int64 whatever the
+    // (finite) coordinates; beyond that the outermost cells are wider
+    const double max_cells = (double)(1 << 30);
     int64_t ncx = 1, ncy = 1;
     if (x1 >= x0) {
-        ncx = (int64_t)(((double)x1 - x0) / cw) + 1;
-        ncy = (int64_t)(((double)y1 - y0) / ch) + 1;
+        ncx = (int64_t)std::min(((double)x1 - x0) / cw, max_cells - 1) + 1;
+        ncy = (int64_t)std::min(((double)y1 - y0) / ch, max_cells - 1) + 1;
     }
     const int64_t ncell = ncx * ncy;           // key ncell: non-finite coordinates
     static thread_local std::vector<int64_t> key;
@@ -124,7 +127,8 @@ void exposure_tiles(const fp_patch_shape &s, int e, int tile_pixels, std::vector
         const float xi = x[i], yi = y[i];
         if (std::isfinite(xi) && std::isfinite(yi)) {
             // offsets are >= 0, so truncation is floor
-            const int64_t cx = (int64_t)(((double)xi - x0) * icw), cy = (int64_t)(((double)yi - y0) * ich);
+            const int64_t cx = (int64_t)std::min(((double)xi - x0) * icw, (double)(ncx - 1));
+            const int64_t cy = (int64_t)std::min(((double)yi - y0) * ich, (double)(ncy - 1));
             key[i] = cy * ncx + cx;
         } else {
             key[i] = ncell;

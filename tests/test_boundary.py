@@ -135,6 +135,21 @@ def test_planner_sparse_and_nonfinite_coordinates():
     assert ti["n_pix"].sum() == p.npix
 
 
+def test_planner_extreme_finite_coordinates():
+    """Coordinates near the float range (cell counts far past int64 if not
+    clamped) still yield every pixel exactly once."""
+    p = S.config_small(seed=1)
+    p.xpix = p.xpix.copy()
+    p.ypix = p.ypix.copy()
+    p.xpix[3] = 3.0e38
+    p.ypix[11] = -3.0e38
+    p.xpix[20] = -1.0e30
+    rc, (sz, ex, ti, bd, od, pm) = plan([p], 256)
+    assert rc == 0
+    assert sorted(pm.tolist()) == list(range(p.npix))
+    assert ti["n_pix"].sum() == p.npix
+
+
 def test_planner_rejects_bad_shapes():
     p = S.config_small(seed=1)
     assert plan([p], 100)[0] == N.FP_ERR_ARGUMENT          # not a multiple of 32
