@@ -2,7 +2,8 @@
 CPU kernel: sources far outside the patch (every Gaussian culled: the model is
 zero, chi2 = sum (d ierr - d ierr)(d ierr + d ierr) = 0 exactly, the gradient
 zero) and extreme shapes (axis ratio 0.21, half-light radii from 0.03" to
-0.6", Sersic indices at both ends of the amplitude table)."""
+0.6", Sersic indices at both ends of the amplitude table), and chunk tails of
+every size in the adjoint."""
 
 import numpy as np
 import pytest
@@ -58,3 +59,24 @@ def test_extreme_shapes(kind, shape):
     tol_c, tol_g = (CHI2_F64, GRAD_F64) if kind == "tiled" else (CHI2_REF, GRAD_REF)
     assert chi2_err(chi2, c64, sc) < tol_c
     assert grad_err(dchi2, g64) < tol_g
+
+
+@pytest.mark.parametrize("n_sources", [1, 2, 3, 4])
+def test_partial_groups_of_every_size(n_sources):
+    """1-Gaussian PSFs (9 image Gaussians per source) on 256-pixel tiles: over
+    these four patches the tiles keep 2 to 30 Gaussians in their last group,
+    so the adjoint replicates it 1, 2, 3, 4, 5, 6 and 8 times.  Tiled results
+    match the FP64 oracle."""
+    from forcepho_b200 import synthetic as S
+    from forcepho_b200.proposal import B200Proposer
+    p = S.config_multiband(seed=90 + n_sources, render=lambda pp, pr: O.render(pp, pr, precision="f64"),
+                           n_sources=n_sources, n_bands=2, exp_per_band=1, size=64, n_psf=1)
+    p.return_residual = True
+    p.send_to_device()
+    prop = p.scene.get_proposal().copy()
+    prop["q"] = np.clip(prop["q"] * 0.97, 0.2, 0.99)
+    chi2, dchi2, res = B200Proposer(tile_pixels=256).evaluate_proposal(prop, patch=p, unpack=False)
+    c64, g64, r64 = O.evaluate(p, prop, precision="f64", return_residual=True)
+    sc = chi2_scale(chi2, p.data, p.ierr, r64)
+    assert chi2_err(chi2, c64, sc) < CHI2_F64
+    assert grad_err(dchi2, g64) < GRAD_F64
