@@ -75,18 +75,24 @@ class B200Proposer(ProposerBase):
         for the autotuned default of the patch's size class.
     ctas_per_sm : persistent CTAs per SM.
     flags : extra ``fp_launch`` flags (e.g. ``FLAG_NO_CULL``).
+    use_graph : replay the proposal upload, the three launches and the read-back
+        of a plan as one CUDA graph (captured on the plan's first call); False
+        issues them one by one.
     """
 
-    def __init__(self, patch=None, tile_pixels=None, ctas_per_sm=4, flags=0):
+    def __init__(self, patch=None, tile_pixels=None, ctas_per_sm=4, flags=0, use_graph=True):
         N.load()
         self.patch = patch
         self.tile_pixels = tile_pixels
         self.ctas_per_sm = ctas_per_sm
         self.flags = flags
+        self.use_graph = use_graph
         self._plan = None
         self._plan_key = None
         self._pinned_prop = None
         self._pinned_out = None
+        self._graph = None
+        self._graph_key = None
 
     def plan_for(self, patch):
         key = (id(patch), patch.plan_signature(), self.tile_pixels)
@@ -95,6 +101,7 @@ class B200Proposer(ProposerBase):
             if tp is None:
                 from .autotune import default_tile_pixels
                 tp = default_tile_pixels(patch)
+            self._graph = None              # captured over the previous plan's buffers
             self._plan = Plan([patch], tile_pixels=tp)
             self._plan_key = key
             self._pinned_prop = torch.zeros(self._plan.proposals.numel(), dtype=torch.uint8).pin_memory()
@@ -115,10 +122,16 @@ class B200Proposer(ProposerBase):
         host = pack_proposals([prop], 1)
         self._pinned_prop.numpy()[:] = host.view(np.uint8).reshape(-1)
         stream = torch.cuda.current_stream()
-        plan.proposals.copy_(self._pinned_prop, non_blocking=True)
-        plan.evaluate(plan.launch(ctas_per_sm=self.ctas_per_sm, flags=self.flags), stream=stream)
-        self._pinned_chi2.copy_(plan.chi2, non_blocking=True)
-        self._pinned_resp.copy_(plan.response, non_blocking=True)
+        lp = plan.launch(ctas_per_sm=self.ctas_per_sm, flags=self.flags)
+        if self.use_graph:
+            gkey = (self._plan_key, self.ctas_per_sm, self.flags)
+            if self._graph is None or self._graph_key != gkey:
+                self._capture(plan, lp, stream)
+                self._graph_key = gkey
+            plan.check_current()
+            self._graph.replay()
+        else:
+            self._queue(plan, lp)
         stream.synchronize()
         chi_out = self._pinned_chi2.numpy()[0, :n_bands].copy()
         chi_derivs = response_view(self._pinned_resp.numpy()[0], n_bands, n_sources).copy()
@@ -128,6 +141,23 @@ class B200Proposer(ProposerBase):
                 residuals = self.unpack_residuals(residuals, patch)
             return chi_out, chi_derivs, residuals
         return chi_out, chi_derivs
+
+    def _queue(self, plan, lp):
+        """Proposal upload, evaluation and read-back on the current stream."""
+        plan.proposals.copy_(self._pinned_prop, non_blocking=True)
+        plan.evaluate(lp)
+        self._pinned_chi2.copy_(plan.chi2, non_blocking=True)
+        self._pinned_resp.copy_(plan.response, non_blocking=True)
+
+    def _capture(self, plan, lp, stream):
+        # one eager pass first sets the kernels' attributes outside the capture
+        self._queue(plan, lp)
+        stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._queue(plan, lp)
+        torch.cuda.synchronize()
+        self._graph = g
 
 
 Proposer = B200Proposer
