@@ -1,11 +1,13 @@
 """Compile the CUDA library ``forcepho_b200/lib/libforcepho_b200.so`` in-tree.
 
-    python -m forcepho_b200.build [--verbose]
+    python -m forcepho_b200.build [--verbose] [--phase-timers]
 
 nvcc builds every ``csrc/*.cu`` for sm_100a only (``-gencode
 arch=compute_100a,code=sm_100a``) into one shared library exporting the C ABI
 of ``include/forcepho_b200.h``.  The library is rebuilt only when a source or
-header is newer than it (or with ``force=True``).
+header is newer than it (or with ``force=True``).  ``--phase-timers`` builds
+the diagnostic variant ``libforcepho_b200_phases.so`` instead (clock64 counters
+at the tile kernel's phase boundaries; ``python -m forcepho_b200.phase_split``).
 """
 
 import glob
@@ -47,12 +49,14 @@ def up_to_date():
     return all(os.path.getmtime(f) <= t for f in _deps())
 
 
-def build(force=False, verbose=False, extra=()):
-    """Build the library if needed; returns its path."""
-    if not force and up_to_date():
+def build(force=False, verbose=False, extra=(), out=None):
+    """Build the library (or, with ``out``, a variant of it at that path) if
+    needed; returns its path."""
+    lib = out or LIB
+    if not force and lib == LIB and up_to_date():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     cmd = [nvcc()] + ARCH + NVCC_FLAGS + list(extra) + ["-o", tmp] + sources() + ["-lcudart"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
@@ -62,11 +66,23 @@ def build(force=False, verbose=False, extra=()):
         sys.stdout.write(r.stdout)
         sys.stderr.write(r.stderr)
     if r.returncode:
-        raise RuntimeError("nvcc failed building %s (exit %d)" % (LIB, r.returncode))
-    os.replace(tmp, LIB)
-    return LIB
+        raise RuntimeError("nvcc failed building %s (exit %d)" % (lib, r.returncode))
+    os.replace(tmp, lib)
+    return lib
+
+
+# diagnostic variant: the tile kernel with per-phase clock64 counters
+# (fp_debug_phases); forcepho_b200.phase_split reports them
+PHASES_LIB = os.path.join(LIBDIR, "libforcepho_b200_phases.so")
+
+
+def build_phase_timers(verbose=False):
+    return build(force=True, verbose=verbose, extra=["-DFP_PHASE_TIMERS"], out=PHASES_LIB)
 
 
 if __name__ == "__main__":
-    build(force=True, verbose="--verbose" in sys.argv)
-    print(LIB)
+    if "--phase-timers" in sys.argv:
+        print(build_phase_timers(verbose="--verbose" in sys.argv))
+    else:
+        build(force=True, verbose="--verbose" in sys.argv)
+        print(LIB)

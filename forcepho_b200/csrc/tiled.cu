@@ -40,6 +40,18 @@
 
 namespace {
 
+#ifdef FP_PHASE_TIMERS
+// Diagnostic build only (libforcepho_b200_phases.so): thread 0 of each CTA
+// reads clock64 at the barriers between the tile kernel's phases, and the
+// per-tile differences are summed here: [1] cull, [2] forward + residual,
+// [3] adjoint, [4] per-tile partials, [5] tiles, [7] all.  The normal build
+// has none of this.
+__device__ unsigned long long g_phase[8];
+#define FP_PHASE_MARK(v) const long long v = clock64()
+#else
+#define FP_PHASE_MARK(v)
+#endif
+
 static_assert(FP_RUN == 32, "the forward pass sums runs of one 32-Gaussian ballot word");
 
 // A chunk's last group of v < 32 Gaussians is replicated min(8, 32 / v) times
@@ -288,6 +300,7 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
         __syncthreads();
         const int ti = s_int[0];
         if (ti < 0) break;
+        FP_PHASE_MARK(ph0);
 
         const fp_tile tl = tiles[ti];
         const fp_exposure_desc ed = expos[tl.expo];
@@ -346,6 +359,7 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
         }
         __syncthreads();
 
+        FP_PHASE_MARK(ph1);
         // ---- 2. forward: model of P pixels per thread ----
         // the tile's pixels are listed in the plan's pixel order (compact cells)
         const int j0 = tid * P;
@@ -509,6 +523,7 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
         }
         for (int t = tid; t < FP_WARPS * MAXSOURCES * NPARAMS; t += FP_THREADS) s_wsrc[t] = 0.0;
 
+        FP_PHASE_MARK(ph2);
         // ---- 3. adjoint: one Gaussian per lane, pixels broadcast ----
         for (int c0 = 0; c0 < (forward_only ? 0 : gc); c0 += FP_CHUNK) {
             const int cn = min(FP_CHUNK, gc - c0);
@@ -605,6 +620,7 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
         }
         __syncthreads();
 
+        FP_PHASE_MARK(ph3);
         // ---- 4. per-tile partials ----
         if (tid == 0) out[0] = s_red[FP_WARPS];
         for (int t = tid; t < ns * NPARAMS; t += FP_THREADS) {
@@ -614,6 +630,18 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
             out[1 + t] = acc;
         }
         // the next iteration's first barrier orders these reads before any reuse
+#ifdef FP_PHASE_TIMERS
+        __syncthreads();
+        if (tid == 0) {
+            const long long ph4 = clock64();
+            atomicAdd(&g_phase[1], (unsigned long long)(ph1 - ph0));
+            atomicAdd(&g_phase[2], (unsigned long long)(ph2 - ph1));
+            atomicAdd(&g_phase[3], (unsigned long long)(ph3 - ph2));
+            atomicAdd(&g_phase[4], (unsigned long long)(ph4 - ph3));
+            atomicAdd(&g_phase[5], 1ULL);
+            atomicAdd(&g_phase[7], (unsigned long long)(ph4 - ph0));
+        }
+#endif
     }
 }
 
@@ -906,3 +934,20 @@ extern "C" int fp_evaluate_batch_noalloc(const fp_patch *const *d_patches, int n
     return fp_evaluate_batch(d_patches, n_patches, sizes, tables, d_proposals, d_chi2, d_response, ws,
                              (size_t)FP_NOALLOC_WORKSPACE_BYTES, launch, stream);
 }
+
+#ifdef FP_PHASE_TIMERS
+// Diagnostic build only: copy the summed phase clocks out (and zero them).
+extern "C" FP_API int fp_debug_phases(unsigned long long out[8], int reset)
+{
+    if (!out) return fp_set_error(FP_ERR_ARGUMENT, "fp_debug_phases: NULL");
+    if (int rc = fp_check_cuda(cudaDeviceSynchronize(), "fp_debug_phases sync")) return rc;
+    if (int rc = fp_check_cuda(cudaMemcpyFromSymbol(out, g_phase, sizeof(unsigned long long) * 8),
+                               "fp_debug_phases copy"))
+        return rc;
+    if (reset) {
+        const unsigned long long z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (int rc = fp_check_cuda(cudaMemcpyToSymbol(g_phase, z, sizeof(z)), "fp_debug_phases reset")) return rc;
+    }
+    return FP_OK;
+}
+#endif
