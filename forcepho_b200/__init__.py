@@ -17,6 +17,7 @@ Modules, with the reference counterparts they stand in for:
   model (``forcepho.sources``, ``forcepho.patches.patch``, ``forcepho.kernel_limits``)
 * ``synthetic``   -- seeded synthetic patches of the benchmark workloads
 * ``build``, ``_native`` -- the in-tree CUDA library and its ctypes bindings
+* ``phase_split`` -- the tile kernel's phase split, from the diagnostic build
 
 Submodules are imported on use; importing the package itself loads nothing.
 """
