@@ -217,25 +217,29 @@ __device__ __forceinline__ void moments_to_grad(const double *__restrict__ J, co
 // (FP32 pixel-loop parameters A = (xc, yc, c Fxx, c Fxy), fys = c Fyy) meets
 // the rectangle [x0,x1] x [y0,y1]: the minimum of the convex quadratic over the
 // rectangle is at the centre if it lies inside, else on an edge, where it is a
-// clamped 1-D minimum.  FP64; non-finite results keep the Gaussian.
+// clamped 1-D minimum.  FP32: near the threshold its rounding error (~1e-4 of
+// E) is far inside the 1% margin (0.36), so no Gaussian with a pixel of the
+// rectangle within the cutoff is dropped; the pair census checks exactly that.
+// Non-finite results keep the Gaussian.
 __device__ __forceinline__ bool ellipse_meets_rect(const float4 A, float fys, float x0, float x1, float y0,
                                                    float y1)
 {
-    const double ic = 1.0 / FP_EXP2_SCALE;
-    const double cx = A.x, cy = A.y, fxx = A.z * ic, fxy = A.w * ic, fyy = fys * ic;
+    const float ic = (float)(1.0 / FP_EXP2_SCALE);
+    const float cx = A.x, cy = A.y, fxx = A.z * ic, fxy = A.w * ic, fyy = fys * ic;
     if (cx >= x0 && cx <= x1 && cy >= y0 && cy <= y1) return true;
-    double best = INFINITY;
-    const double lx = x0 - cx, hx = x1 - cx, ly = y0 - cy, hy = y1 - cy;
+    const float rxx = __frcp_rn(fxx), ryy = __frcp_rn(fyy);
+    float best = INFINITY;
+    const float lx = x0 - cx, hx = x1 - cx, ly = y0 - cy, hy = y1 - cy;
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
-        const double dx = k ? hx : lx;
-        const double dy = fmin(fmax(-fxy * dx / fyy, ly), hy);
-        best = fmin(best, fxx * dx * dx + 2.0 * fxy * dx * dy + fyy * dy * dy);
-        const double ey = k ? hy : ly;
-        const double ex = fmin(fmax(-fxy * ey / fxx, lx), hx);
-        best = fmin(best, fxx * ex * ex + 2.0 * fxy * ex * ey + fyy * ey * ey);
+        const float dx = k ? hx : lx;
+        const float dy = fminf(fmaxf(-fxy * dx * ryy, ly), hy);
+        best = fminf(best, fmaf(fxx * dx, dx, fmaf(2.f * fxy * dx, dy, fyy * dy * dy)));
+        const float ey = k ? hy : ly;
+        const float ex = fminf(fmaxf(-fxy * ey * rxx, lx), hx);
+        best = fminf(best, fmaf(fxx * ex, ex, fmaf(2.f * fxy * ex, ey, fyy * ey * ey)));
     }
-    return !(best > MAX_EXP_ARG * 1.01);
+    return !(best > (float)(MAX_EXP_ARG * 1.01));
 }
 
 struct tile_smem {
