@@ -67,7 +67,9 @@ class PatchFarm:
     weights : per-patch work estimates (e.g. pixel-Gaussian pairs)
     rank, world : this process and the number of processes
     evaluator : callable(list of local patches) -> callable(list of proposals)
-        -> list of results; defaults to a ``BatchedProposer`` on this rank's GPU
+        -> list of results; defaults to a ``BatchedProposer`` on the current
+        CUDA device, so each rank selects its GPU first
+        (``torch.cuda.set_device(local_rank)``)
     """
 
     def __init__(self, make_patch, weights, rank, world, evaluator=None):
