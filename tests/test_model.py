@@ -7,7 +7,8 @@ on the CPU, with the FP64 oracle standing in for the device proposer:
   q, pa, sersic, rhalf] per source, shape terms summed over bands;
 * ``FastPosterior``: lnp = -chi2/2 + log|J| and its gradient through the
   transform, the Sersic-amplitude splines and the proposal, against central
-  differences of lnp; the position cache.
+  differences of lnp; the position cache;
+* ``optimize_one_band``: the weighted linear flux solve.
 """
 
 import numpy as np
@@ -97,3 +98,20 @@ def test_fastposterior_lnp_terms_and_cache():
     chi2, _ = O.evaluate(post.patch, post.scene.get_proposal(), precision="f64")[:2]
     want = -0.5 * chi2.sum() + post.transform.lndetjac(z0)
     assert lnp == pytest.approx(want, rel=1e-12, abs=1e-9)
+
+
+def test_optimize_one_band_recovers_fluxes():
+    """The weighted flux solve (forcepho/fitting.py:572-587): noiseless data
+    X^T f give back f, and the precision matrix is X_w X_w^T."""
+    from forcepho_b200.fitting import optimize_one_band
+    rng = np.random.default_rng(11)
+    X = np.abs(rng.normal(size=(4, 300)))
+    f = np.array([3.0, 0.5, 12.0, 7.0])
+    w = rng.uniform(0.5, 2.0, 300)
+    y = f @ X
+    flux, prec = optimize_one_band(X, w, y)
+    np.testing.assert_allclose(flux[:, 0], f, rtol=1e-10)
+    np.testing.assert_allclose(prec, (X * w) @ (X * w).T, rtol=1e-12)
+    # a fixed-source model is subtracted first
+    flux2, _ = optimize_one_band(X, w, y + 2.0, fixedX=2.0)
+    np.testing.assert_allclose(flux2[:, 0], f, rtol=1e-10)
