@@ -672,13 +672,16 @@ def run_nuts_bench(args):
     z, lnp, g = nuts.state                 # the adapted chains continue into the kept transitions
     torch.cuda.synchronize()
     ev0 = nuts.n_evals
-    t1 = time.perf_counter()
+    props_dev = torch.cuda.get_device_properties(0)
+    gpu_id = ("GPU-" + str(props_dev.uuid)) if getattr(props_dev, "uuid", None) else "0"
     stats = []
-    for _ in range(args.steps):
-        z, lnp, g, st = nuts.iterate(z, lnp, g, tune=False)
-        stats.append(st)
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t1
+    with ClockSampler(gpu_id) as clk:
+        t1 = time.perf_counter()
+        for _ in range(args.steps):
+            z, lnp, g, st = nuts.iterate(z, lnp, g, tune=False)
+            stats.append(st)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t1
     evals = nuts.n_evals - ev0
     live_leaves = float(sum(st["n_steps"].sum() for st in stats))
     pairs = h.plan.n_pairs * evals
@@ -694,7 +697,7 @@ def run_nuts_bench(args):
            "tree_depth_mean": float(np.mean([st["depth"] for st in stats])),
            "mean_tree_accept": float(np.mean([st["mean_tree_accept"] for st in stats])),
            "divergences": int(sum(st["diverging"].sum() for st in stats)),
-           "setup_s": setup_s, "warmup_s": warm_s}
+           "clocks": clk.summary(), "setup_s": setup_s, "warmup_s": warm_s}
     print(json.dumps(out), flush=True)
 
 
