@@ -45,6 +45,13 @@ def test_library_exports_every_declared_symbol():
     assert set(syms) == set(N.SIGNATURES), "binding signatures and header disagree"
 
 
+def test_normal_library_has_no_phase_timers():
+    """The clock64 phase counters exist only in the diagnostic build
+    (``python -m forcepho_b200.build --phase-timers``)."""
+    L = N.load()
+    assert not hasattr(L, "fp_debug_phases")
+
+
 def test_struct_sizes_reported_by_library():
     L = N.load()
     out = np.zeros(4, np.int32)
