@@ -217,10 +217,11 @@ __device__ __forceinline__ void moments_to_grad(const double *__restrict__ J, co
 // (FP32 pixel-loop parameters A = (xc, yc, c Fxx, c Fxy), fys = c Fyy) meets
 // the rectangle [x0,x1] x [y0,y1]: the minimum of the convex quadratic over the
 // rectangle is at the centre if it lies inside, else on an edge, where it is a
-// clamped 1-D minimum.  FP32: near the threshold the Gaussian lies within a
-// few pixels of the rectangle, so the offsets x0 - cx, ... are exact (Sterbenz;
-// coordinates within a factor 2 of each other), and the quadratic form's
-// rounding error (~1e-4 of E) is far inside the 1% margin (0.36).  No
+// clamped 1-D minimum.  FP32: near the threshold the centre lies within the
+// Gaussian's cutoff radius of the rectangle, so the offsets x0 - cx, ... are
+// exact wherever the coordinates exceed that radius (Sterbenz: within a factor
+// 2 of each other) and round below 1e-5 px where they do not; the quadratic
+// form's rounding error (~1e-4 of E) is far inside the 1% margin (0.36).  No
 // Gaussian with a pixel of the rectangle within the cutoff is dropped; the
 // pair census checks exactly that.  Non-finite results keep the Gaussian.
 __device__ __forceinline__ bool ellipse_meets_rect(const float4 A, float fys, float x0, float x1, float y0,
