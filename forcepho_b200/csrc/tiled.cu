@@ -220,8 +220,9 @@ __device__ __forceinline__ void moments_to_grad(const double *__restrict__ J, co
 // clamped 1-D minimum.  FP32: near the threshold the centre lies within the
 // Gaussian's cutoff radius of the rectangle, so the offsets x0 - cx, ... are
 // exact wherever the coordinates exceed that radius (Sterbenz: within a factor
-// 2 of each other) and round below 1e-5 px where they do not; the quadratic
-// form's rounding error (~1e-4 of E) is far inside the 1% margin (0.36).  No
+// 2 of each other); where they do not, the coordinates are small and an offset
+// error d moves E by only about 12 d / sigma.  The quadratic form's rounding
+// error (~1e-4 of E) is far inside the 1% margin (0.36) as well.  No
 // Gaussian with a pixel of the rectangle within the cutoff is dropped; the
 // pair census checks exactly that.  Non-finite results keep the Gaussian.
 __device__ __forceinline__ bool ellipse_meets_rect(const float4 A, float fys, float x0, float x1, float y0,
