@@ -57,6 +57,9 @@ FLAG_STATIC = 2
 FLAG_FORWARD_ONLY = 4
 PHASE_SETUP, PHASE_TILES, PHASE_REDUCE = 1, 2, 4
 
+# device status word bits (include/forcepho_b200.h)
+STATUS_TILE_SIZE, STATUS_GAUSS_COUNT, STATUS_SOURCES = 1, 2, 4
+
 # return codes (include/forcepho_b200.h)
 FP_OK, FP_ERR_ARGUMENT, FP_ERR_LIMITS, FP_ERR_CUDA, FP_ERR_WORKSPACE, FP_ERR_DEVICE = 0, -1, -2, -3, -4, -5
 
@@ -87,6 +90,7 @@ SIGNATURES = {
                                                  ctypes.POINTER(PlanTables), c_vp, c_vp, c_vp,
                                                  ctypes.POINTER(Launch), c_vp]),
     "fp_read_status": (ctypes.c_int, [c_vp, ctypes.POINTER(c_i32), c_vp]),
+    "fp_read_status_noalloc": (ctypes.c_int, [ctypes.POINTER(c_i32), c_vp]),
     "fp_count_pairs": (ctypes.c_int, [c_vp, ctypes.POINTER(PlanSizes), ctypes.POINTER(PlanTables), c_vp, c_sz,
                                       c_vp, c_vp]),
     "fp_hmc_prepare": (ctypes.c_int, [c_vp, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),

@@ -25,11 +25,7 @@ int fp_sm_count(int *out);
 #define FP_CHUNK 256                // Gaussians staged in shared memory at a time
 #define FP_RUN 32                   // FP32 run length before flushing to FP64
 
-// ---- device status word bits ----------------------------------------------
-#define FP_STATUS_TILE_SIZE   1     // a tile larger than the launch's tile size
-#define FP_STATUS_GAUSS_COUNT 2     // an exposure with more Gaussians than planned
-#define FP_STATUS_SOURCES     4     // n_sources above MAXSOURCES or inconsistent
-#define FP_STATUS_BAND        8     // band index out of range
+// device status word bits: FP_STATUS_* in include/forcepho_b200.h
 
 // ---- workspace layout (tiled path) -----------------------------------------
 // [0, 256)                        : control block (queue counter, status)

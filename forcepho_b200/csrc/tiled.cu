@@ -71,7 +71,19 @@ setup_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc
     const fp_exposure_desc ed = expos[blockIdx.x];
     const fp_patch *pt = patches[ed.patch];
     if (ed.n_sources > MAXSOURCES || pt->n_sources != ed.n_sources) {
+        // the patch no longer matches the plan: report it, and make every
+        // Gaussian of the exposure inert (zero amplitude and Jacobian, a box
+        // that meets no pixel), so that whatever an earlier evaluation left in
+        // the tables cannot reach this one's results
         if (threadIdx.x == 0) atomicOr(&ctl->status, FP_STATUS_SOURCES);
+        for (int g = threadIdx.x; g < ed.n_gauss; g += blockDim.x) {
+            const int64_t i = ed.gauss_offset + g;
+            gfwd[2 * i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            gfwd[2 * i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+            gbox[i] = make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY);
+            double *J = gjac + (size_t)FP_JAC * i;
+            for (int k = 0; k < FP_JAC; ++k) J[k] = 0.0;
+        }
         return;
     }
     const fp_source *srcs = proposals + (size_t)ed.patch * MAXSOURCES;
@@ -818,28 +830,38 @@ extern "C" int fp_count_pairs(const fp_patch *const *d_patches, const fp_plan_si
     return fp_check_cuda(cudaGetLastError(), "count_kernel launch");
 }
 
-extern "C" int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches, const fp_plan_sizes *sizes,
-                                 const fp_plan_tables *tables, const fp_source *d_proposals, double *d_chi2,
-                                 fp_response *d_response, void *d_workspace, size_t workspace_bytes,
-                                 const fp_launch *launch, void *stream)
+namespace {
+
+// What a validated batched evaluation needs to launch.
+struct batch_launch {
+    fp_workspace_layout L;
+    int tile_pixels;
+    size_t smem;
+    int n_sm;
+};
+
+// Argument checks shared by fp_evaluate_batch and fp_evaluate_batch_noalloc:
+// everything but the workspace pointer, so that a rejected call has no side
+// effects (no launch, no write to any buffer).
+int check_batch(const fp_patch *const *d_patches, int n_patches, const fp_plan_sizes *sizes,
+                const fp_plan_tables *tables, const fp_source *d_proposals, const double *d_chi2,
+                const fp_response *d_response, size_t workspace_bytes, const fp_launch *launch, const char *who,
+                batch_launch *out)
 {
-    if (!d_patches || n_patches < 1 || !sizes || !d_proposals || !d_chi2 || !d_response || !d_workspace ||
-        !launch)
-        return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch: NULL argument");
-    if (int rc = check_tables(tables, "fp_evaluate_batch")) return rc;
-    const fp_plan_tables &tb = *tables;
-    if (((uintptr_t)d_workspace) & 255)
-        return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch: workspace must be 256-byte aligned");
+    if (!d_patches || n_patches < 1 || !sizes || !d_proposals || !d_chi2 || !d_response || !launch)
+        return fp_set_error(FP_ERR_ARGUMENT, "%s: NULL argument", who);
+    if (int rc = check_tables(tables, who)) return rc;
     const fp_workspace_layout L = fp_layout(sizes->n_gauss, sizes->n_partials);
     if (workspace_bytes < L.total)
-        return fp_set_error(FP_ERR_WORKSPACE, "fp_evaluate_batch: workspace %zu B < required %zu B",
-                            workspace_bytes, L.total);
+        return fp_set_error(FP_ERR_WORKSPACE, "%s: workspace %zu B < required %zu B", who, workspace_bytes,
+                            L.total);
     const int T = launch->tile_pixels;
     if (T != 256 && T != 512 && T != 1024)
-        return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch: tile_pixels=%d (supported: 256, 512, 1024)", T);
+        return fp_set_error(FP_ERR_ARGUMENT, "%s: tile_pixels=%d (supported: 256, 512, 1024)", who, T);
     if (sizes->max_gauss > 65535)
-        return fp_set_error(FP_ERR_LIMITS, "fp_evaluate_batch: %lld image Gaussians in one exposure (max 65535)",
+        return fp_set_error(FP_ERR_LIMITS, "%s: %lld image Gaussians in one exposure (max 65535)", who,
                             (long long)sizes->max_gauss);
+    if (sizes->n_exposures > INT32_MAX) return fp_set_error(FP_ERR_LIMITS, "%s: too many exposures", who);
     const size_t smem = tile_smem_layout(T, (int)sizes->max_gauss).total;
     int dev = 0, optin = 0, nsm = 0;
     if (int rc = fp_check_cuda(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
@@ -847,28 +869,37 @@ extern "C" int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches
                                "cudaDeviceGetAttribute"))
         return rc;
     if (smem > (size_t)optin)
-        return fp_set_error(FP_ERR_LIMITS, "fp_evaluate_batch: tile needs %zu B shared memory (limit %d B)", smem,
-                            optin);
+        return fp_set_error(FP_ERR_LIMITS, "%s: tile needs %zu B shared memory (limit %d B)", who, smem, optin);
     if (int rc = fp_sm_count(&nsm)) return rc;
+    out->L = L;
+    out->tile_pixels = T;
+    out->smem = smem;
+    out->n_sm = nsm;
+    return FP_OK;
+}
 
-    unsigned char *ws = reinterpret_cast<unsigned char *>(d_workspace);
+// The three launches of an evaluation (arguments already checked).
+int run_batch(const batch_launch &a, const fp_patch *const *d_patches, const fp_plan_sizes *sizes,
+              const fp_plan_tables &tb, const fp_source *d_proposals, double *d_chi2, fp_response *d_response,
+              unsigned char *ws, const fp_launch *launch, cudaStream_t st)
+{
+    const fp_workspace_layout &L = a.L;
+    const int T = a.tile_pixels;
     fp_control *ctl = reinterpret_cast<fp_control *>(ws);
     float4 *gfwd = reinterpret_cast<float4 *>(ws + L.gauss_fwd);
     float4 *gbox = reinterpret_cast<float4 *>(ws + L.gauss_box);
     double *gjac = reinterpret_cast<double *>(ws + L.gauss_jac);
     double *partials = reinterpret_cast<double *>(ws + L.partials);
-    cudaStream_t st = (cudaStream_t)stream;
 
     const int phases = launch->phases ? launch->phases : (FP_PHASE_SETUP | FP_PHASE_TILES | FP_PHASE_REDUCE);
     if ((phases & FP_PHASE_SETUP) && sizes->n_exposures > 0) {
-        if (sizes->n_exposures > INT32_MAX) return fp_set_error(FP_ERR_LIMITS, "too many exposures");
         setup_kernel<<<(unsigned)sizes->n_exposures, 256, 0, st>>>(d_patches, tb.expos, d_proposals, gfwd, gbox,
                                                                    gjac, ctl);
         if (int rc = fp_check_cuda(cudaGetLastError(), "setup_kernel launch")) return rc;
     }
     if ((phases & FP_PHASE_TILES) && sizes->n_tiles > 0) {
         const int cps = launch->ctas_per_sm > 0 ? launch->ctas_per_sm : 2;
-        const int64_t want = (int64_t)cps * nsm;
+        const int64_t want = (int64_t)cps * a.n_sm;
         const int grid = (int)(want < sizes->n_tiles ? want : sizes->n_tiles);
         // the persistent CTAs pop tiles from this counter
         if (int rc = fp_check_cuda(cudaMemsetAsync(&ctl->queue, 0, sizeof(ctl->queue), st), "queue reset"))
@@ -876,13 +907,13 @@ extern "C" int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches
         int rc;
         const int mg = (int)sizes->max_gauss;
         if (T == 256)
-            rc = launch_tiles<1>(grid, smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gjac, partials, ctl,
+            rc = launch_tiles<1>(grid, a.smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gjac, partials, ctl,
                                  mg, launch->flags);
         else if (T == 512)
-            rc = launch_tiles<2>(grid, smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gjac, partials, ctl,
+            rc = launch_tiles<2>(grid, a.smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gjac, partials, ctl,
                                  mg, launch->flags);
         else
-            rc = launch_tiles<4>(grid, smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gjac, partials, ctl,
+            rc = launch_tiles<4>(grid, a.smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gjac, partials, ctl,
                                  mg, launch->flags);
         if (rc) return rc;
     }
@@ -892,6 +923,24 @@ extern "C" int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches
         if (int rc = fp_check_cuda(cudaGetLastError(), "reduce_kernel launch")) return rc;
     }
     return FP_OK;
+}
+
+}  // namespace
+
+extern "C" int fp_evaluate_batch(const fp_patch *const *d_patches, int n_patches, const fp_plan_sizes *sizes,
+                                 const fp_plan_tables *tables, const fp_source *d_proposals, double *d_chi2,
+                                 fp_response *d_response, void *d_workspace, size_t workspace_bytes,
+                                 const fp_launch *launch, void *stream)
+{
+    if (!d_workspace) return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch: NULL workspace");
+    if (((uintptr_t)d_workspace) & 255)
+        return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch: workspace must be 256-byte aligned");
+    batch_launch a;
+    if (int rc = check_batch(d_patches, n_patches, sizes, tables, d_proposals, d_chi2, d_response, workspace_bytes,
+                             launch, "fp_evaluate_batch", &a))
+        return rc;
+    return run_batch(a, d_patches, sizes, *tables, d_proposals, d_chi2, d_response,
+                     reinterpret_cast<unsigned char *>(d_workspace), launch, (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -909,6 +958,28 @@ static __device__ __align__(256) unsigned char g_noalloc_ws[FP_NOALLOC_WORKSPACE
 namespace {
 constexpr int NOALLOC_MAX_DEVICES = 64;
 std::atomic<void *> g_noalloc_addr[NOALLOC_MAX_DEVICES];
+
+// The array's device address on the current device.  Its name in host code is
+// only a host-side stand-in, so the address is looked up (cudaGetSymbolAddress,
+// with the device current) on the first call on each device and kept.  The
+// kept address belongs to the device's primary context at that time:
+// cudaDeviceReset destroys that context, and a process that resets a device
+// must not call these entry points on it afterwards.
+int noalloc_address(const char *who, void **out)
+{
+    int dev = 0;
+    if (int rc = fp_check_cuda(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return fp_set_error(FP_ERR_ARGUMENT, "%s: device %d beyond %d", who, dev, NOALLOC_MAX_DEVICES);
+    void *ws = g_noalloc_addr[dev].load();
+    if (ws == nullptr) {
+        if (int rc = fp_check_cuda(cudaGetSymbolAddress(&ws, g_noalloc_ws), "cudaGetSymbolAddress(noalloc workspace)"))
+            return rc;
+        g_noalloc_addr[dev].store(ws);
+    }
+    *out = ws;
+    return FP_OK;
+}
 }  // namespace
 
 extern "C" int fp_evaluate_batch_noalloc(const fp_patch *const *d_patches, int n_patches,
@@ -916,31 +987,35 @@ extern "C" int fp_evaluate_batch_noalloc(const fp_patch *const *d_patches, int n
                                          const fp_source *d_proposals, double *d_chi2, fp_response *d_response,
                                          const fp_launch *launch, void *stream)
 {
-    if (!sizes) return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch_noalloc: NULL sizes");
+    const char *who = "fp_evaluate_batch_noalloc";
+    if (!sizes) return fp_set_error(FP_ERR_ARGUMENT, "%s: NULL sizes", who);
     if (sizes->workspace_bytes < 0 || (uint64_t)sizes->workspace_bytes > (uint64_t)FP_NOALLOC_WORKSPACE_BYTES)
         return fp_set_error(FP_ERR_WORKSPACE,
-                            "fp_evaluate_batch_noalloc: the plan needs %lld B of workspace, more than the fixed "
-                            "%llu B array; use fp_evaluate_batch with a caller-allocated workspace",
-                            (long long)sizes->workspace_bytes, (unsigned long long)FP_NOALLOC_WORKSPACE_BYTES);
-    int dev = 0;
-    if (int rc = fp_check_cuda(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
-    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
-        return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_batch_noalloc: device %d beyond %d", dev,
-                            NOALLOC_MAX_DEVICES);
-    // set-up, once per device, with that device current: the array's device
-    // address (its name in host code is only a host-side stand-in)
-    void *ws = g_noalloc_addr[dev].load();
-    if (ws == nullptr) {
-        if (int rc = fp_check_cuda(cudaGetSymbolAddress(&ws, g_noalloc_ws), "cudaGetSymbolAddress(noalloc workspace)"))
-            return rc;
-        g_noalloc_addr[dev].store(ws);
-    }
-    // the control block (work-queue counter, status word) must start at zero
+                            "%s: the plan needs %lld B of workspace, more than the fixed %llu B array; use "
+                            "fp_evaluate_batch with a caller-allocated workspace",
+                            who, (long long)sizes->workspace_bytes, (unsigned long long)FP_NOALLOC_WORKSPACE_BYTES);
+    // every check first: a rejected call touches neither the array nor the stream
+    batch_launch a;
+    if (int rc = check_batch(d_patches, n_patches, sizes, tables, d_proposals, d_chi2, d_response,
+                             (size_t)FP_NOALLOC_WORKSPACE_BYTES, launch, who, &a))
+        return rc;
+    void *ws = nullptr;
+    if (int rc = noalloc_address(who, &ws)) return rc;
+    // the control block (work-queue counter, status word) must start at zero;
+    // the status word then describes this call alone (fp_read_status_noalloc)
     if (int rc = fp_check_cuda(cudaMemsetAsync(ws, 0, sizeof(fp_control), (cudaStream_t)stream),
                                "fp_evaluate_batch_noalloc: clear control block"))
         return rc;
-    return fp_evaluate_batch(d_patches, n_patches, sizes, tables, d_proposals, d_chi2, d_response, ws,
-                             (size_t)FP_NOALLOC_WORKSPACE_BYTES, launch, stream);
+    return run_batch(a, d_patches, sizes, *tables, d_proposals, d_chi2, d_response,
+                     reinterpret_cast<unsigned char *>(ws), launch, (cudaStream_t)stream);
+}
+
+extern "C" int fp_read_status_noalloc(int32_t *status_out, void *stream)
+{
+    if (!status_out) return fp_set_error(FP_ERR_ARGUMENT, "fp_read_status_noalloc: NULL");
+    void *ws = nullptr;
+    if (int rc = noalloc_address("fp_read_status_noalloc", &ws)) return rc;
+    return fp_read_status(ws, status_out, stream);
 }
 
 #ifdef FP_PHASE_TIMERS

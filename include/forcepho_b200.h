@@ -120,6 +120,14 @@ typedef struct fp_response {
 #define FP_ERR_WORKSPACE   -4   /* workspace smaller than required */
 #define FP_ERR_DEVICE      -5   /* a kernel reported an inconsistency in its status word */
 
+/* Bits of the device status word of the batched kernels (fp_read_status).  A
+ * tile or exposure that sets one contributes nothing to the results: a
+ * rejected exposure renders a zero model with a zero gradient, a rejected
+ * tile adds zero partial sums. */
+#define FP_STATUS_TILE_SIZE   1 /* a tile larger than the launch's tile size */
+#define FP_STATUS_GAUSS_COUNT 2 /* an exposure with more image Gaussians than the plan's maximum */
+#define FP_STATUS_SOURCES     4 /* the patch struct's n_sources differs from the plan's, or exceeds MAXSOURCES */
+
 /* One-line description of the most recent error on the calling thread. */
 FP_API const char *fp_error_string(void);
 
@@ -408,13 +416,17 @@ FP_API int fp_hmc_leapfrog(const fp_hmc_patch *d_hp, int n_patches, const fp_hmc
  * sizes->workspace_bytes exceed it are rejected with FP_ERR_WORKSPACE (a
  * single patch of 30 sources x 8 bands x 4 exposures of 256x256 pixels needs
  * about 15 MB; a 512-patch batch does not fit).  The caller still passes all
- * inputs and outputs; nothing is allocated or freed.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress) with that
- * device current, so make that first call before any stream capture.  All
- * calls share the array and it keeps the previous call's contents (the call
- * clears the part that must start at zero): calls that overlap on the GPU, on
- * different streams or from different threads, race and corrupt each other's
- * results. */
+ * inputs and outputs; nothing is allocated or freed.  Arguments are checked
+ * before anything is queued, so a rejected call leaves the array and the
+ * stream untouched.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current and keeps it, so
+ * make that first call before any stream capture; the kept address belongs to
+ * the device's primary context, so a process that calls cudaDeviceReset on a
+ * device must not use this entry point on it afterwards.  All calls share the
+ * array and it keeps the previous call's contents (each call clears the part
+ * that must start at zero, including the status word): calls that overlap on
+ * the GPU, on different streams or from different threads, race and corrupt
+ * each other's results. */
 FP_API int fp_evaluate_batch_noalloc(const fp_patch *const *d_patches, int n_patches,
                                      const fp_plan_sizes *sizes, const fp_plan_tables *tables,
                                      const fp_source *d_proposals,
@@ -422,8 +434,18 @@ FP_API int fp_evaluate_batch_noalloc(const fp_patch *const *d_patches, int n_pat
                                      void *stream);
 
 /* Read and clear the device status word written by the batched kernels
- * (0 = no inconsistency seen).  Synchronises `stream`. */
+ * (0 = no inconsistency seen; FP_STATUS_* bits otherwise).  Synchronises
+ * `stream`. */
 FP_API int fp_read_status(void *d_workspace, int32_t *status_out, void *stream);
+
+/* fp_read_status for the fixed array of fp_evaluate_batch_noalloc: the
+ * FP_STATUS_* bits of the last fp_evaluate_batch_noalloc call on the current
+ * device (each call clears them at its start), then cleared.  Call it on the
+ * stream of that call; it synchronises `stream`.  A call whose patch no longer
+ * matches its plan reports FP_STATUS_SOURCES here and returns a zero model
+ * (chi2 0, gradient 0) for the exposures concerned.  No counterpart in the
+ * reference; it allocates nothing either. */
+FP_API int fp_read_status_noalloc(int32_t *status_out, void *stream);
 
 #ifdef __cplusplus
 }

@@ -38,13 +38,27 @@ _lib = None
 _ref = None
 
 
+def reference_root():
+    """Where the reference's sources lie: $FORCEPHO_REF_ROOT, else the default
+    REF_ROOT of oracle/Makefile (the one place that names it)."""
+    env = os.environ.get("FORCEPHO_REF_ROOT")
+    if env:
+        return env
+    import re
+    with open(os.path.join(HERE, "Makefile")) as f:
+        m = re.search(r"^REF_ROOT\s*\?=\s*(\S+)", f.read(), re.M)
+    return m.group(1) if m else ""
+
+
 def build(force=False):
     """Compile the oracle (and the reference kernel when its sources exist)."""
     import subprocess
     targets = ["oracle"]
-    if os.path.isdir("/root/reference/forcepho/src"):
+    root = reference_root()
+    if root and os.path.isdir(os.path.join(root, "forcepho", "src")):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + (["-B"] if force else []) + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE] + (["-B"] if force else []) + targets + ["REF_ROOT=" + root],
+                   check=True)
 
 
 def lib():

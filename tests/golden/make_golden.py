@@ -71,7 +71,7 @@ def outputs(patch, proposals):
 
 def slow_path_model(patch, proposal, band=0, exposure=0):
     """Model pixels of one exposure from forcepho/slow/gaussmodel.py (FP64)."""
-    path = "/root/reference/forcepho/slow/gaussmodel.py"
+    path = os.path.join(O.reference_root(), "forcepho", "slow", "gaussmodel.py")
     spec = importlib.util.spec_from_file_location("fp_slow_gaussmodel", path)
     gm = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(gm)

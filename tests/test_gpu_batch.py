@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tolerances import CHI2_F64, GRAD_F64, chi2_err, chi2_scale, grad_err
+from tolerances import CHI2_F64, GRAD_F64, band_scales, chi2_err, chi2_raw_err, chi2_scale, grad_err
 
 pytestmark = pytest.mark.gpu
 
@@ -56,6 +56,7 @@ def test_batch_matches_oracle_and_single_patch(batch):
         c64, g64, r64 = O.evaluate(p, prop, precision="f64", return_residual=True)
         scale = chi2_scale(chi2, p.data, p.ierr, r64)
         assert chi2_err(chi2, c64, scale) < CHI2_F64
+        assert chi2_raw_err(chi2, c64, band_scales(p, r64)) < CHI2_F64
         assert grad_err(dchi2, g64) < GRAD_F64
         c1, g1 = single.evaluate_proposal(prop, patch=p)
         np.testing.assert_array_equal(chi2, c1)
@@ -190,4 +191,5 @@ def test_shuffled_pixels_and_plan_without_coordinates():
     c64, g64, r64 = O.evaluate(p, prop, precision="f64", return_residual=True)
     sc = chi2_scale(chi2, p.data, p.ierr, r64)
     assert chi2_err(chi2, c64, sc) < CHI2_F64
+    assert chi2_raw_err(chi2, c64, band_scales(p, r64)) < CHI2_F64
     assert grad_err(dchi2, g64) < GRAD_F64

@@ -7,7 +7,8 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tolerances import CHI2_F64, CHI2_REF, GRAD_F64, GRAD_REF, chi2_err, chi2_scale, grad_err
+from tolerances import (CHI2_F64, CHI2_REF, GRAD_F64, GRAD_REF, band_scales, chi2_err, chi2_raw_err, chi2_scale,
+                        grad_err, ref_gap_explained)
 
 pytestmark = pytest.mark.gpu
 
@@ -37,6 +38,8 @@ def test_max_bands_and_sources(kind):
     assert grad_err(dchi2, gr) < GRAD_REF
     tol_c, tol_g = (CHI2_F64, GRAD_F64) if kind == "tiled" else (CHI2_REF, GRAD_REF)
     assert chi2_err(chi2, c64, sc) < tol_c
+    assert chi2_raw_err(chi2, c64, band_scales(p, r64)) < tol_c
+    assert ref_gap_explained(chi2, cr, c64, tol_c)
     assert grad_err(dchi2, g64) < tol_g
     scale = float(np.max(np.abs(r64)))
     assert np.max(np.abs(res.astype(np.float64) - r64)) <= 1e-5 * scale

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tolerances import CHI2_F64, GRAD_F64, chi2_err, chi2_scale, grad_err
+from tolerances import CHI2_F64, GRAD_F64, band_scales, chi2_err, chi2_raw_err, chi2_scale, grad_err
 
 pytestmark = pytest.mark.gpu
 
@@ -84,6 +84,7 @@ def test_subtract_fixed_matches_sequential_blocks():
     c64, g64, r64 = O.evaluate(q, scene.get_proposal(), precision="f64", return_residual=True)
     sc = chi2_scale(chi2, q.data, q.ierr, r64)
     assert chi2_err(chi2, c64, sc) < CHI2_F64
+    assert chi2_raw_err(chi2, c64, band_scales(q, r64)) < CHI2_F64
     assert grad_err(dchi2, g64) < GRAD_F64
 
 

@@ -9,7 +9,8 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tolerances import CHI2_F64, CHI2_REF, GRAD_F64, GRAD_REF, chi2_err, chi2_scale, grad_err
+from tolerances import (CHI2_F64, CHI2_REF, GRAD_F64, GRAD_REF, band_scales, chi2_err, chi2_raw_err, chi2_scale,
+                        grad_err, ref_gap_explained)
 
 pytestmark = pytest.mark.gpu
 
@@ -58,6 +59,8 @@ def test_extreme_shapes(kind, shape):
     assert grad_err(dchi2, gr) < GRAD_REF
     tol_c, tol_g = (CHI2_F64, GRAD_F64) if kind == "tiled" else (CHI2_REF, GRAD_REF)
     assert chi2_err(chi2, c64, sc) < tol_c
+    assert chi2_raw_err(chi2, c64, band_scales(p, r64)) < tol_c
+    assert ref_gap_explained(chi2, cr, c64, tol_c)
     assert grad_err(dchi2, g64) < tol_g
 
 
@@ -79,4 +82,5 @@ def test_partial_groups_of_every_size(n_sources):
     c64, g64, r64 = O.evaluate(p, prop, precision="f64", return_residual=True)
     sc = chi2_scale(chi2, p.data, p.ierr, r64)
     assert chi2_err(chi2, c64, sc) < CHI2_F64
+    assert chi2_raw_err(chi2, c64, band_scales(p, r64)) < CHI2_F64
     assert grad_err(dchi2, g64) < GRAD_F64
