@@ -72,7 +72,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "limits", "multiband", "small", "hmc", "nuts"])
+    ap.add_argument("--workload", default="batched",
+                    choices=["batched", "limits", "multiband", "small", "hmc", "nuts", "single", "precision"])
     ap.add_argument("--nuts-depth", type=int, default=6, help="max tree depth (nuts workload)")
     ap.add_argument("--hmc-steps", type=int, default=16, help="leapfrog steps per trajectory (hmc workload)")
     ap.add_argument("--patches", type=int, default=512)
@@ -468,7 +469,8 @@ def run_ours(args):
         p.send_to_device()
     proposals = perturbed_proposals(patches)
     tp = args.tile_pixels or 1024
-    bp = BatchedProposer(patches, tile_pixels=tp, autotune=not args.no_autotune and not args.tile_pixels)
+    tune = "classes" if not args.no_autotune and not args.tile_pixels else False
+    bp = BatchedProposer(patches, tile_pixels=tp, autotune=tune)
     bp.set_proposals_async(proposals)
     torch.cuda.synchronize()
     setup_s = time.perf_counter() - t_setup
@@ -619,6 +621,7 @@ def run_ours(args):
                "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                "config": config_of(args, len(patches), {"tile_pixels": bp.tile_pixels,
+                                                        "tile_classes": bp.tile_classes,
                                                         "ctas_per_sm": bp.launch.ctas_per_sm,
                                                         "pairs_per_step_per_gpu": n_pairs,
                                                         "parallelism": "replicas-%d (independent patch batches)"
@@ -640,12 +643,19 @@ def run_hmc(args):
     """Device-resident HMC on patches of the limits distribution (30 sources,
     8 bands x 4 exposures of 256x256 px, 6-Gaussian PSFs): --patches of them
     (128 unless given), --hmc-steps leapfrog steps per trajectory, --warmup
-    adapting trajectories, then --steps timed trajectories (CUDA-graph replays)."""
+    adapting trajectories (dual-averaging step sizes per patch; the diagonal
+    mass matrix re-estimated from the draws of the warm-up's second half, then
+    the step sizes adapted again), then --steps timed trajectories
+    (CUDA-graph replays).  Precision study (CPU leg, untimed): at seeded chain
+    positions recorded during the timed trajectories (device copies), chi2 and
+    every gradient component of seeded patches against the FP64 oracle and the
+    reference CPU kernel at the same proposals."""
     import torch
     from forcepho_b200 import synthetic as S
     from forcepho_b200.batch import render_models
     from forcepho_b200.hmc import DeviceHMC
     from forcepho_b200.proposal import B200Proposer
+    from forcepho_b200.structs import source_struct_dtype
     torch.cuda.set_device(0)
     n = 128 if args.patches == 512 else args.patches
     rng = np.random.default_rng(5)
@@ -661,13 +671,32 @@ def run_hmc(args):
         th = p.scene.get_all_source_params().reshape(int(p.n_sources), -1).copy()
         th[:, :p.n_bands] *= r.uniform(0.9, 1.1, th[:, :p.n_bands].shape)   # start off the truth
         theta0.append(th.reshape(-1))
-    n_traj = args.warmup + args.steps + 2
+    n_final = max(10, args.warmup // 4)          # step-size adaptation after the mass-matrix update
+    n_traj = args.warmup + n_final + args.steps + 2
     h = DeviceHMC(patches, theta0, n_steps=args.hmc_steps, max_traj=n_traj, step_size=0.05)
     h.estimate_inv_mass()
     setup_s = time.perf_counter() - t0
-    h.run(args.warmup, adapt=True)
+    # warm-up: step sizes, then the mass matrix from the second half's draws, then step sizes again
+    tw = time.perf_counter()
+    w1 = args.warmup // 2
+    h.run(w1, adapt=True, target=0.8)
+    h.end_adaptation()
+    w2 = args.warmup - w1
+    draws = torch.zeros((w2, h.n_params), dtype=torch.float64, device=h.device)
+    h.run(w2, adapt=True, target=0.8, record={t: draws[t] for t in range(w2)})
+    h.end_adaptation()
+    if w2 >= 10:
+        h.adapt_mass_from(draws)
+        h.start_adaptation(0.8)
+        h.run(n_final, adapt=True, target=0.8)
+        h.end_adaptation()
     torch.cuda.synchronize()
+    warm_s = time.perf_counter() - tw
     acc0 = h.accepted.clone()
+    # seeded chain positions to check (trajectory index within the timed run)
+    prng = np.random.default_rng(17)
+    rec_t = sorted(set(int(t) for t in prng.integers(0, max(args.steps, 1), 4)))
+    record = {t: torch.zeros(h.n_params, dtype=torch.float64, device=h.device) for t in rec_t}
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     props_dev = torch.cuda.get_device_properties(0)
@@ -675,7 +704,7 @@ def run_hmc(args):
     with ClockSampler(gpu_id) as clk:
         torch.cuda.nvtx.range_push("bench_timed")
         e0.record(stream)
-        h.run(args.steps)
+        h.run(args.steps, record=record)
         e1.record(stream)
         e1.synchronize()
         torch.cuda.nvtx.range_pop()
@@ -684,34 +713,62 @@ def run_hmc(args):
     pairs = h.plan.n_pairs * args.hmc_steps * args.steps
     acc = ((h.accepted - acc0).double() / args.steps).cpu().numpy()
     de = h.energy_error.cpu().numpy()
+    eps = h.eps.cpu().numpy()
     out = {"metric": METRIC, "value": pairs / (ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
            "config": {"workload": "hmc", "patches": n, "leapfrog_steps": args.hmc_steps,
+                      "trajectories_timed": args.steps,
                       "patch": "30 sources, 8 bands x 4 exposures of 256x256 px, 6-Gaussian PSFs",
-                      "mass_matrix": "diagonal, Hessian-diagonal estimate (8 Hutchinson probes)",
+                      "mass_matrix": "diagonal: Hessian-diagonal estimate, then the variance of the warm-up's "
+                                     "second-half draws",
+                      "step_size": "per patch, dual averaging towards acceptance 0.8 during warm-up, averaged "
+                                   "step size after",
                       "step": "a trajectory of every patch (graph replay)"},
            "gradient_evals_per_s": grad_evals / (ms * 1e-3),
            "trajectories_per_s": n * args.steps / (ms * 1e-3),
-           "acceptance_mean": float(acc.mean()), "energy_error_abs_median": float(np.median(np.abs(de))),
-           "clocks": clk.summary(), "setup_s": setup_s, "gpu_launches": args.steps * (6 * args.hmc_steps + 2)}
+           "acceptance_mean": float(acc.mean()), "acceptance_min": float(acc.min()),
+           "energy_error_abs_median": float(np.median(np.abs(de))),
+           "step_size_median": float(np.median(eps)), "step_size_range": [float(eps.min()), float(eps.max())],
+           "clocks": clk.summary(), "setup_s": setup_s, "warmup_s": warm_s,
+           "gpu_launches": args.steps * (6 * args.hmc_steps + 2)}
     if not args.no_cpu:
-        # CPU leg (checker, untimed): patch 0 at its final position vs the FP64
-        # oracle and the reference CPU kernel, two bands
         from oracle import oracle as O
-        p = patches[0]
-        h.positions()                       # proposals at the current (accepted) positions
-        props = h.proposals()[0][:int(p.n_sources)].copy()
-        chi2, dchi2 = B200Proposer().evaluate_proposal(props, patch=p)
-        prec = {}
-        for name, fn in (("vs_f64", lambda: O.evaluate(p, props, precision="f64", bands=(0, 4))),
-                         ("vs_reference", lambda: O.ref_evaluate(p, props, bands=(0, 4)))):
-            c, g, _ = fn()
-            prec[name] = {"chi2_relerr_max": float(max(abs(chi2[b] - c[b]) / abs(c[b]) for b in (0, 4))),
-                          "grad_colnorm_relerr_max": float(max(
-                              np.linalg.norm(dchi2[b][..., k] - g[b][..., k]) / np.linalg.norm(g[b][..., k])
-                              for b in (0, 4) for k in range(7) if np.linalg.norm(g[b][..., k]) > 0))}
-        out["precision"] = dict(prec, patch=0, bands=[0, 4], state="final HMC position")
+        # proposals at the recorded positions (device splines and transform), for
+        # seeded patches; GPU results from the proposer on those exact records
+        picks = sorted(set(int(i) for i in prng.integers(0, n, 3)))
+        rows = []
+        worst = {"gpu_vs_f64": [0.0, 0.0, 0.0], "gpu_vs_reference": [0.0, 0.0, 0.0],
+                 "reference_vs_f64": [0.0, 0.0, 0.0]}
+        bands = (0, 5)
+        for t in rec_t:
+            h.z.copy_(record[t])
+            h.positions()
+            props_all = h.proposals()
+            for i in picks:
+                p = patches[i]
+                prop = np.ascontiguousarray(props_all[i][:int(p.n_sources)]).view(source_struct_dtype)
+                chi2, dchi2 = B200Proposer().evaluate_proposal(prop, patch=p)
+                c64, g64, r64 = O.evaluate(p, prop, precision="f64", return_residual=True, bands=bands)
+                cref, gref, _ = O.ref_evaluate(p, prop, bands=bands)
+                vals = {"gpu": (chi2, dchi2), "f64": (c64, g64), "reference": (cref, gref)}
+                row = {"trajectory": t, "patch": i}
+                for key, (a, b) in (("gpu_vs_f64", ("gpu", "f64")), ("gpu_vs_reference", ("gpu", "reference")),
+                                    ("reference_vs_f64", ("reference", "f64"))):
+                    ca, ga = vals[a]
+                    cb, gb = vals[b]
+                    cre = max(abs(ca[bb] - cb[bb]) / abs(cb[bb]) for bb in bands)
+                    cols = component_errors(np.asarray(ga)[list(bands)], np.asarray(gb)[list(bands)])
+                    gn = max(c["norm"] for c in cols)
+                    gc = max(c["comp_max"] for c in cols)
+                    row[key] = {"chi2_relerr": cre, "grad_colnorm": gn, "grad_comp_max": gc}
+                    w = worst[key]
+                    w[0], w[1], w[2] = max(w[0], cre), max(w[1], gn), max(w[2], gc)
+                rows.append(row)
+        out["precision"] = {"positions": rows, "bands": list(bands),
+                            "worst": {k: {"chi2_relerr": v[0], "grad_colnorm": v[1], "grad_comp_max": v[2]}
+                                      for k, v in worst.items()},
+                            "state": "chain positions recorded during the timed trajectories"}
     print(json.dumps(out), flush=True)
 
 
@@ -782,6 +839,142 @@ def run_nuts_bench(args):
     print(json.dumps(out), flush=True)
 
 
+def run_single(args):
+    """Single-patch call latency, as forcepho's own samplers call the kernel
+    (one proposal per call, host proposal in, results out): the Python
+    proposer (one CUDA-graph replay per call), the reference's kernel ABI
+    (fp_evaluate_proposal: struct and index-array read-backs, then the tiled
+    launches on the library's cached plan) and the plain comparator, on the
+    small (64x64 px, one source) and multiband (16 sources, 5 bands x 2
+    exposures of 150x150 px) patches.  --steps calls per path after --warmup."""
+    import ctypes
+    import torch
+    from forcepho_b200 import _native as N
+    from forcepho_b200 import synthetic as S
+    from forcepho_b200.kernel_limits import MAXSOURCES, NPARAMS
+    from forcepho_b200.proposal import B200Proposer, PlainProposer
+    torch.cuda.set_device(0)
+    L = N.load()
+    steps = max(args.steps, 50)
+    out = {"metric": "single-patch lnlike+grad call latency", "unit": "us per call", "steps": steps,
+           "warmup": args.warmup, "higher_is_better": False, "data": "synthetic", "patches": {}}
+    for name in ("small", "multiband"):
+        p = S.CONFIGS[name](seed=1)
+        p.return_residual = False
+        p.send_to_device()
+        prop = perturbed_proposals([p])[0]
+        nb, ns = p.n_bands, int(p.n_sources)
+        pin_prop = torch.from_numpy(prop.view(np.uint8).copy()).pin_memory()
+        d_prop = torch.empty_like(pin_prop, device="cuda")
+        d_chi2 = torch.zeros(nb, dtype=torch.float64, device="cuda")
+        d_resp = torch.zeros((nb, MAXSOURCES * NPARAMS), dtype=torch.float32, device="cuda")
+        h_chi2 = torch.zeros(nb, dtype=torch.float64).pin_memory()
+        h_resp = torch.zeros((nb, MAXSOURCES * NPARAMS), dtype=torch.float32).pin_memory()
+        stream = torch.cuda.current_stream()
+
+        def abi_call():
+            d_prop.copy_(pin_prop, non_blocking=True)
+            N.check(L.fp_evaluate_proposal(p.device_patch_ptr, d_prop.data_ptr(), ns, nb, d_chi2.data_ptr(),
+                                           d_resp.data_ptr(), ctypes.c_void_p(stream.cuda_stream)),
+                    "fp_evaluate_proposal")
+            h_chi2.copy_(d_chi2, non_blocking=True)
+            h_resp.copy_(d_resp, non_blocking=True)
+            stream.synchronize()
+
+        tiled, plain = B200Proposer(), PlainProposer()
+        paths = {"proposer_graph": lambda: tiled.evaluate_proposal(prop, patch=p),
+                 "reference_abi": abi_call,
+                 "plain": lambda: plain.evaluate_proposal(prop, patch=p)}
+        res = {}
+        for key, fn in paths.items():
+            for _ in range(max(args.warmup, 3)):
+                fn()
+            t = time.perf_counter()
+            for _ in range(steps):
+                fn()
+            res[key] = 1e6 * (time.perf_counter() - t) / steps
+        res["pairs"] = int(p.n_pairs())
+        out["patches"][name] = res
+    print(json.dumps(out), flush=True)
+
+
+def component_errors(g, gref, rel_floor=1e-3):
+    """Per parameter column k: the normwise error ||g - gref|| / ||gref|| and
+    the largest and median error of single components |g - gref| / |gref|
+    over the components with |gref| >= rel_floor * max |gref| of the column."""
+    g = np.asarray(g, np.float64)
+    gref = np.asarray(gref, np.float64)
+    out = []
+    for k in range(gref.shape[-1]):
+        a, b = g[..., k].ravel(), gref[..., k].ravel()
+        den = np.linalg.norm(b)
+        if den == 0:
+            out.append({"norm": 0.0, "comp_max": 0.0, "comp_median": 0.0})
+            continue
+        big = np.abs(b) >= rel_floor * np.abs(b).max()
+        ce = np.abs(a[big] - b[big]) / np.abs(b[big])
+        out.append({"norm": float(np.linalg.norm(a - b) / den), "comp_max": float(ce.max()),
+                    "comp_median": float(np.median(ce))})
+    return out
+
+
+def run_precision(args):
+    """Error of the loaded library against the FP64 oracle: chi2 (raw,
+    per band) and every gradient component, on the limits-size patch (two
+    bands) and on a seeded spread of the batched workload's patches.  Run once
+    per precision variant (FORCEPHO_B200_VARIANT unset: FP32 runs flushed to
+    FP64; =kahan: FP32 + Kahan) on the same inputs."""
+    import torch
+    from forcepho_b200 import synthetic as S
+    from forcepho_b200 import _native as N
+    from forcepho_b200.proposal import B200Proposer
+    from oracle import oracle as O
+    torch.cuda.set_device(0)
+    N.load()
+    variant = os.environ.get("FORCEPHO_B200_VARIANT", "") or "fp32-runs-flushed-to-fp64"
+    cases = []
+    lim = S.config_limits(seed=3)
+    cases.append(("limits", lim, perturbed_proposals([lim])[0], (0, 4)))
+    shapes = S.batched_shapes(seed=4, n_patches=args.patches)
+    pats = []
+    for sh in shapes:
+        rng = np.random.default_rng(sh["seed"])
+        p = S.make_patch(rng, n_sources=sh["n_sources"], exp_per_band=sh["exp_per_band"], exp_pix=sh["exp_pix"],
+                         n_psf=4, source_params=S._broad_source, raster_width=256)
+        p._rng = rng
+        pats.append(p)
+    for i in precision_sample(pats, 4, max_pairs=2e9):
+        p = pats[i]
+        S.add_noise(p, p._rng, p._rng.uniform(0.5, 2.0, p.n_exp), O.render(p, p.scene.get_proposal()))
+        cases.append(("batched[%d]" % i, p, perturbed_proposals([p])[0], None))
+    rows = []
+    worst = {"chi2_relerr": 0.0, "grad_norm": 0.0, "grad_comp_max": 0.0}
+    for name, p, prop, bands in cases:
+        p.return_residual = False
+        p.send_to_device()
+        chi2, dchi2 = B200Proposer().evaluate_proposal(prop, patch=p)
+        c64, g64, r64 = O.evaluate(p, prop, precision="f64", return_residual=True, bands=bands)
+        bl = list(range(p.n_bands)) if bands is None else list(bands)
+        sc = []
+        for b in bl:
+            e0, ne = int(p.band_start[b]), int(p.band_N[b])
+            s0 = int(p.exposure_start[e0])
+            s1 = int(p.exposure_start[e0 + ne - 1] + p.exposure_N[e0 + ne - 1])
+            d = p.data[s0:s1].astype(np.float64) * p.ierr[s0:s1]
+            r = r64[s0:s1] * p.ierr[s0:s1]
+            sc.append(float(np.sum(d * d + r * r)))
+        ce = [abs(chi2[b] - c64[b]) / max(abs(c64[b]), 1e-3 * s_) for b, s_ in zip(bl, sc)]
+        cols = component_errors(dchi2[bl], g64[bl])
+        rows.append({"patch": name, "pairs": int(p.n_pairs()), "bands": bl, "chi2_relerr": ce,
+                     "grad": dict(zip(["flux", "ra", "dec", "q", "pa", "sersic", "rhalf"], cols))})
+        worst["chi2_relerr"] = max(worst["chi2_relerr"], max(ce))
+        worst["grad_norm"] = max(worst["grad_norm"], max(c["norm"] for c in cols))
+        worst["grad_comp_max"] = max(worst["grad_comp_max"], max(c["comp_max"] for c in cols))
+        p.free()
+    print(json.dumps({"metric": "error vs FP64 oracle", "variant": variant, "library": N.lib_path(),
+                      "worst": worst, "cases": rows}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -790,6 +983,10 @@ def main():
         run_hmc(args)
     elif args.workload == "nuts":
         run_nuts_bench(args)
+    elif args.workload == "single":
+        run_single(args)
+    elif args.workload == "precision":
+        run_precision(args)
     else:
         run_ours(args)
 

@@ -29,7 +29,26 @@ class PlanSizes(ctypes.Structure):
 
 
 class PlanTables(ctypes.Structure):
-    _fields_ = [("expos", c_vp), ("tiles", c_vp), ("order", c_vp), ("bands", c_vp), ("perm", c_vp)]
+    _fields_ = [("expos", c_vp), ("tiles", c_vp), ("order", c_vp), ("bands", c_vp), ("perm", c_vp),
+                ("pix", c_vp)]
+
+
+class TileRule(ctypes.Structure):
+    _fields_ = [("n_classes", c_i32), ("max_exposure_pixels", c_i32 * 4), ("tile_pixels", c_i32 * 4)]
+
+
+def tile_rule(classes):
+    """TileRule from [(max_exposure_pixels, tile_pixels), ...] (ascending; the
+    last class's bound is ignored: it takes every larger exposure)."""
+    classes = list(classes)
+    if not 1 <= len(classes) <= 4:
+        raise ValueError("1 to 4 tile classes")
+    r = TileRule()
+    r.n_classes = len(classes)
+    for c, (mx, tp) in enumerate(classes):
+        r.max_exposure_pixels[c] = int(min(mx, 2 ** 31 - 1))
+        r.tile_pixels[c] = int(tp)
+    return r
 
 
 class Launch(ctypes.Structure):
@@ -68,7 +87,7 @@ exposure_desc_dtype = np.dtype([("gauss_offset", np.int64), ("patch", np.int32),
                                 ("band", np.int32), ("n_gauss", np.int32), ("n_psf", np.int32),
                                 ("n_sources", np.int32)])
 tile_dtype = np.dtype([("partial_offset", np.int64), ("expo", np.int32), ("perm_start", np.int32),
-                       ("n_pix", np.int32), ("pad", np.int32), ("bbox", np.float32, 4)])
+                       ("n_pix", np.int32), ("tile_pixels", np.int32), ("bbox", np.float32, 4)])
 band_desc_dtype = np.dtype([("patch", np.int32), ("band", np.int32), ("tile_begin", np.int32),
                             ("tile_end", np.int32), ("n_sources", np.int32), ("pad", np.int32)])
 assert exposure_desc_dtype.itemsize == 32 and tile_dtype.itemsize == 40 and band_desc_dtype.itemsize == 24
@@ -80,9 +99,14 @@ SIGNATURES = {
     "fp_struct_sizes": (ctypes.c_int, [c_vp]),
     "fp_evaluate_proposal_plain": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp]),
     "fp_evaluate_proposal": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp]),
+    "fp_evaluate_proposal_release": (ctypes.c_int, []),
     "fp_plan_count": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PlanSizes)]),
     "fp_plan_fill": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "fp_plan_count_rule": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.POINTER(TileRule), ctypes.POINTER(PlanSizes)]),
+    "fp_plan_fill_rule": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.POINTER(TileRule), c_vp, c_vp, c_vp, c_vp,
+                                         c_vp]),
     "fp_plan_bbox": (ctypes.c_int, [c_vp, ctypes.POINTER(PlanSizes), ctypes.POINTER(PlanTables), c_vp]),
+    "fp_plan_pack": (ctypes.c_int, [c_vp, ctypes.POINTER(PlanSizes), ctypes.POINTER(PlanTables), c_vp, c_vp]),
     "fp_tile_smem_bytes": (ctypes.c_int, [ctypes.c_int, c_i64, ctypes.POINTER(c_i64)]),
     "fp_evaluate_batch": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.POINTER(PlanSizes), ctypes.POINTER(PlanTables),
                                          c_vp, c_vp, c_vp, c_vp, c_sz, ctypes.POINTER(Launch), c_vp]),
@@ -110,7 +134,7 @@ _lib = None
 
 
 def lib_path():
-    return _build.LIB
+    return _build.variant_lib() if _build.LIB == _build.DEFAULT_LIB else _build.LIB
 
 
 def load(build_if_missing=True):
@@ -118,11 +142,12 @@ def load(build_if_missing=True):
     global _lib
     if _lib is not None:
         return _lib
-    if build_if_missing:
+    path = lib_path()
+    if build_if_missing and path == _build.DEFAULT_LIB:
         _build.build()
-    if not os.path.exists(_build.LIB):
-        raise NativeError("CUDA library %s is missing; run python -m forcepho_b200.build" % _build.LIB)
-    L = ctypes.CDLL(_build.LIB)
+    if not os.path.exists(path):
+        raise NativeError("CUDA library %s is missing; run python -m forcepho_b200.build" % path)
+    L = ctypes.CDLL(path)
     for name, (res, args) in SIGNATURES.items():
         f = getattr(L, name)
         f.restype = res
@@ -131,7 +156,7 @@ def load(build_if_missing=True):
     L.fp_struct_sizes(sizes.ctypes.data)
     want = [STRUCT_SIZES["patch"], STRUCT_SIZES["source"], STRUCT_SIZES["response"], STRUCT_SIZES["psf"]]
     if list(sizes) != want:
-        raise NativeError("struct sizes of %s are %s, expected %s" % (_build.LIB, list(sizes), want))
+        raise NativeError("struct sizes of %s are %s, expected %s" % (path, list(sizes), want))
     _lib = L
     return L
 

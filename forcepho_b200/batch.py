@@ -43,7 +43,7 @@ class BatchedProposer:
     """
 
     def __init__(self, patches, tile_pixels=1024, ctas_per_sm=4, flags=0, autotune=False,
-                 use_graph=True, tuner=None):
+                 use_graph=True, tuner=None, tile_classes=None):
         N.load()
         self.patches = list(patches)
         self.n = len(self.patches)
@@ -53,9 +53,9 @@ class BatchedProposer:
         self.tune_log = []
         if autotune:
             tuner = tuner or Autotuner()
-            self._autotune(tuner)
+            self._autotune(tuner, per_class=autotune == "classes")
         else:
-            self.plan = Plan(self.patches, tile_pixels=tile_pixels)
+            self.plan = Plan(self.patches, tile_pixels=tile_pixels, tile_classes=tile_classes)
             self.launch = self.plan.launch(ctas_per_sm=ctas_per_sm, flags=flags)
         self._init_host_buffers()
 
@@ -89,21 +89,33 @@ class BatchedProposer:
         self._d2h_done = None
 
     # --- launch parameters ---
-    def _autotune(self, tuner):
+    def _autotune(self, tuner, per_class=False):
+        """Time the candidates and keep the fastest: one tile size for the
+        plan, or (``per_class``) one per exposure-size class."""
         props = self._current_proposals()
 
-        def make_plan(tp):
-            pl = Plan(self.patches, tile_pixels=tp)
+        def make_plan(tp=None, classes=None):
+            pl = Plan(self.patches, tile_pixels=tp or 1024, tile_classes=classes)
             pl.proposals.copy_(torch.from_numpy(props.view(np.uint8).reshape(-1)))
             return pl
 
         n_pairs = sum(p.n_pairs() for p in self.patches)
         key = size_class(n_pairs, sum(p.npix for p in self.patches) // 1024)
-        tp, cps, ms = tuner.tune(key, make_plan)
-        self.tune_log = [r for r in tuner.log if r[0] == key]
-        self.plan = Plan(self.patches, tile_pixels=tp)
+        if per_class:
+            classes, cps, ms = tuner.tune_classes(key, lambda cl: make_plan(classes=cl))
+            self.tune_log = [r for r in tuner.log if r[0][1:] == key]
+            self.plan = Plan(self.patches, tile_classes=classes)
+        else:
+            tp, cps, ms = tuner.tune(key, make_plan)
+            self.tune_log = [r for r in tuner.log if r[0] == key]
+            self.plan = Plan(self.patches, tile_pixels=tp)
         self.launch = self.plan.launch(ctas_per_sm=cps, flags=self.flags)
         self.plan.proposals.copy_(torch.from_numpy(props.view(np.uint8).reshape(-1)))
+
+    @property
+    def tile_classes(self):
+        """[(max exposure pixels, tile pixels), ...] of the plan (one class when uniform)."""
+        return self.plan.tile_classes or [(2 ** 31 - 1, self.plan.tile_pixels)]
 
     def _current_proposals(self):
         return pack_proposals([p.scene.get_proposal() if getattr(p, "scene", None) is not None
@@ -125,7 +137,8 @@ class BatchedProposer:
         their copy to the device."""
         if len(proposals) > self.n:
             raise ValueError("%d proposals for %d patches" % (len(proposals), self.n))
-        self.plan.check_current()            # a captured graph replays the plan's tables
+        s = stream or torch.cuda.current_stream()
+        self.plan.check_current(s)           # a captured graph replays the plan's tables
         if self._h2d_done is not None:
             self._h2d_done.synchronize()     # the previous copy may still read the buffer
         slots, lens = self._prop_slots, self._prop_len
@@ -144,7 +157,6 @@ class BatchedProposer:
             if k < lens[i]:
                 slots[i, k:lens[i]] = _ZERO_RECORD
             lens[i] = k
-        s = stream or torch.cuda.current_stream()
         with torch.cuda.stream(s):
             self.plan.proposals.copy_(self._pin_prop, non_blocking=True)
         self._h2d_done = torch.cuda.Event()
@@ -153,6 +165,7 @@ class BatchedProposer:
     def run(self, stream=None):
         """Queue one evaluation of the device proposals (graph replay when captured)."""
         s = stream or torch.cuda.current_stream()
+        self.plan.check_current(s)           # raises on a stale plan, re-packs swapped data
         if self.use_graph:
             if self.graph is None:
                 self.capture(s)

@@ -20,6 +20,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libforcepho_b200.so")
+DEFAULT_LIB = LIB
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -80,9 +81,33 @@ def build_phase_timers(verbose=False):
     return build(force=True, verbose=verbose, extra=["-DFP_PHASE_TIMERS"], out=PHASES_LIB)
 
 
+# precision variant: per-thread FP32 + Kahan sums in the pixel loops (model,
+# chi2 terms, adjoint moments) instead of FP32 runs flushed to FP64; the
+# comparison of the two schemes (bench.py --workload precision) loads it with
+# FORCEPHO_B200_VARIANT=kahan
+KAHAN_LIB = os.path.join(LIBDIR, "libforcepho_b200_kahan.so")
+
+
+def build_kahan(verbose=False):
+    return build(force=True, verbose=verbose, extra=["-DFP_KAHAN"], out=KAHAN_LIB)
+
+
+def variant_lib():
+    """The library _native loads: the normal build, or the variant named by
+    $FORCEPHO_B200_VARIANT ("kahan")."""
+    v = os.environ.get("FORCEPHO_B200_VARIANT", "")
+    if v == "kahan":
+        return KAHAN_LIB
+    if v:
+        raise ValueError("FORCEPHO_B200_VARIANT=%r: known variants are 'kahan'" % v)
+    return LIB
+
+
 if __name__ == "__main__":
     if "--phase-timers" in sys.argv:
         print(build_phase_timers(verbose="--verbose" in sys.argv))
+    elif "--kahan" in sys.argv:
+        print(build_kahan(verbose="--verbose" in sys.argv))
     else:
         build(force=True, verbose="--verbose" in sys.argv)
         print(LIB)

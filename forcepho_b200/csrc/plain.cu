@@ -194,41 +194,3 @@ extern "C" int fp_evaluate_proposal_plain(const fp_patch *d_patch, const fp_sour
                                                                         d_response);
     return fp_check_cuda(cudaGetLastError(), "plain_kernel launch");
 }
-
-extern "C" int fp_evaluate_proposal(const fp_patch *d_patch, const fp_source *d_sources, int n_sources,
-                                    int n_bands, double *d_chi2, fp_response *d_response, void *stream)
-{
-    if (!d_patch || !d_sources || !d_chi2 || !d_response)
-        return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_proposal: NULL pointer");
-    if (n_bands < 1 || n_bands > MAXBANDS)
-        return fp_set_error(FP_ERR_LIMITS, "fp_evaluate_proposal: n_bands=%d outside [1,%d]", n_bands, MAXBANDS);
-    if (n_sources < 0 || n_sources > MAXSOURCES)
-        return fp_set_error(FP_ERR_LIMITS, "fp_evaluate_proposal: n_sources=%d outside [0,%d]", n_sources,
-                            MAXSOURCES);
-    cudaStream_t st = (cudaStream_t)stream;
-    fp_patch hp;
-    if (int rc = fp_check_cuda(cudaMemcpyAsync(&hp, d_patch, sizeof(fp_patch), cudaMemcpyDeviceToHost, st),
-                               "fp_evaluate_proposal: read patch struct"))
-        return rc;
-    if (int rc = fp_check_cuda(cudaStreamSynchronize(st), "fp_evaluate_proposal: stream")) return rc;
-    if (hp.n_sources != n_sources)
-        return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_proposal: n_sources=%d but the patch has %d", n_sources,
-                            hp.n_sources);
-    if (!hp.n_psf_per_source)
-        return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_proposal: patch without n_psf_per_source");
-    int32_t npsf[MAXBANDS];
-    if (int rc = fp_check_cuda(cudaMemcpyAsync(npsf, hp.n_psf_per_source, sizeof(int32_t) * n_bands,
-                                               cudaMemcpyDeviceToHost, st),
-                               "fp_evaluate_proposal: read n_psf_per_source"))
-        return rc;
-    if (int rc = fp_check_cuda(cudaStreamSynchronize(st), "fp_evaluate_proposal: stream")) return rc;
-    int64_t max_psf = 0;
-    for (int b = 0; b < n_bands; ++b) {
-        if (npsf[b] <= 0)
-            return fp_set_error(FP_ERR_ARGUMENT, "fp_evaluate_proposal: n_psf_per_source[%d]=%d", b, npsf[b]);
-        max_psf = npsf[b] > max_psf ? npsf[b] : max_psf;
-    }
-    const int64_t max_gauss = (int64_t)n_sources * max_psf;
-    if (max_gauss > INT32_MAX) return fp_set_error(FP_ERR_LIMITS, "fp_evaluate_proposal: too many Gaussians");
-    return fp_evaluate_proposal_plain(d_patch, d_sources, n_bands, (int)max_gauss, d_chi2, d_response, stream);
-}

@@ -9,7 +9,9 @@
 // Tiles are spatially compact: each exposure's pixels are grouped into square
 // cells of the image plane (32x32 pixels for 1024-pixel tiles, 32x16 for 512,
 // 16x16 for 256), cells ordered row by row, pixels within a cell kept in their
-// input order.  The plan's pixel order (`perm`) lists, tile after tile, the
+// input order.  The tile size may differ between exposures (a tile rule of up
+// to FP_MAX_TILE_CLASSES classes by exposure pixel count); each tile records
+// its class, and one persistent launch evaluates tiles of every class.  The plan's pixel order (`perm`) lists, tile after tile, the
 // index of every pixel within its patch.  A compact tile has a small bounding
 // box, so the per-tile culling of image Gaussians keeps few that do not reach
 // its pixels.  Without coordinates (xpix == NULL) tiles are runs of
@@ -67,6 +69,35 @@ int check_tile_pixels(int tile_pixels)
         return fp_set_error(FP_ERR_ARGUMENT, "tile_pixels=%d must be a multiple of 32 in [32, 4096]",
                             tile_pixels);
     return FP_OK;
+}
+
+int check_rule(const fp_tile_rule *r)
+{
+    if (!r || r->n_classes < 1 || r->n_classes > FP_MAX_TILE_CLASSES)
+        return fp_set_error(FP_ERR_ARGUMENT, "tile rule: n_classes must be in [1, %d]", FP_MAX_TILE_CLASSES);
+    for (int c = 0; c < r->n_classes; ++c) {
+        if (int rc = check_tile_pixels(r->tile_pixels[c])) return rc;
+        if (c > 0 && c < r->n_classes - 1 && r->max_exposure_pixels[c] < r->max_exposure_pixels[c - 1])
+            return fp_set_error(FP_ERR_ARGUMENT, "tile rule: class bounds must ascend");
+    }
+    return FP_OK;
+}
+
+fp_tile_rule single_class(int tile_pixels)
+{
+    fp_tile_rule r = {};
+    r.n_classes = 1;
+    r.max_exposure_pixels[0] = INT32_MAX;
+    r.tile_pixels[0] = tile_pixels;
+    return r;
+}
+
+// Tile size of an exposure of n pixels: the first class whose bound holds it.
+int rule_tile(const fp_tile_rule &r, int n)
+{
+    for (int c = 0; c < r.n_classes - 1; ++c)
+        if (n <= r.max_exposure_pixels[c]) return r.tile_pixels[c];
+    return r.tile_pixels[r.n_classes - 1];
 }
 
 // cell width x height (pixels) of a tile size: the squarest power-of-two
@@ -164,27 +195,30 @@ void exposure_tiles(const fp_patch_shape &s, int e, int tile_pixels, std::vector
 struct patch_plan {
     std::vector<int32_t> tile_n;      // tile sizes, canonical order
     std::vector<int32_t> tile_expo;   // exposure (within the patch) of each tile
+    std::vector<int32_t> tile_cls;    // size class (tile_pixels) of each tile
     std::vector<int32_t> perm;        // pixel order (indices within the patch)
     int rc = FP_OK;
 };
 
-void plan_one(const fp_patch_shape &s, int p, int tile_pixels, bool want_order, patch_plan &out)
+void plan_one(const fp_patch_shape &s, int p, const fp_tile_rule &rule, bool want_order, patch_plan &out)
 {
     out.rc = check_shape(s, p);
     if (out.rc) return;
     std::vector<int32_t> order, tile_n;
     for (int b = 0; b < s.n_bands; ++b)
         for (int e = s.band_start[b]; e < s.band_start[b] + s.band_N[b]; ++e) {
-            exposure_tiles(s, e, tile_pixels, want_order ? &order : nullptr, tile_n);
+            const int tp = rule_tile(rule, s.exposure_N[e]);
+            exposure_tiles(s, e, tp, want_order ? &order : nullptr, tile_n);
             out.tile_n.insert(out.tile_n.end(), tile_n.begin(), tile_n.end());
             out.tile_expo.insert(out.tile_expo.end(), tile_n.size(), e);
+            out.tile_cls.insert(out.tile_cls.end(), tile_n.size(), tp);
             if (want_order)
                 for (int32_t k : order) out.perm.push_back(s.exposure_start[e] + k);
         }
 }
 
 // Phase 1 over all patches on the host's cores.
-int plan_all(const fp_patch_shape *h_shapes, int n_patches, int tile_pixels, bool want_order,
+int plan_all(const fp_patch_shape *h_shapes, int n_patches, const fp_tile_rule &rule, bool want_order,
              std::vector<patch_plan> &plans)
 {
     plans.assign((size_t)n_patches, patch_plan());
@@ -192,7 +226,7 @@ int plan_all(const fp_patch_shape *h_shapes, int n_patches, int tile_pixels, boo
     nt = std::min<unsigned>(nt, (unsigned)n_patches);
     std::atomic<int> next(0);
     auto work = [&]() {
-        for (int p = next++; p < n_patches; p = next++) plan_one(h_shapes[p], p, tile_pixels, want_order, plans[p]);
+        for (int p = next++; p < n_patches; p = next++) plan_one(h_shapes[p], p, rule, want_order, plans[p]);
     };
     std::vector<std::thread> pool;
     for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
@@ -235,26 +269,43 @@ int count_from(const fp_patch_shape *h_shapes, int n_patches, const std::vector<
 
 }  // namespace
 
+extern "C" int fp_plan_count_rule(const fp_patch_shape *h_shapes, int n_patches, const fp_tile_rule *rule,
+                                  fp_plan_sizes *out)
+{
+    if (!h_shapes || !out || n_patches < 1) return fp_set_error(FP_ERR_ARGUMENT, "fp_plan_count: bad arguments");
+    if (int rc = check_rule(rule)) return rc;
+    std::vector<patch_plan> plans;
+    if (int rc = plan_all(h_shapes, n_patches, *rule, false, plans)) return rc;
+    return count_from(h_shapes, n_patches, plans, out);
+}
+
 extern "C" int fp_plan_count(const fp_patch_shape *h_shapes, int n_patches, int tile_pixels,
                              fp_plan_sizes *out)
 {
-    if (!h_shapes || !out || n_patches < 1) return fp_set_error(FP_ERR_ARGUMENT, "fp_plan_count: bad arguments");
     if (int rc = check_tile_pixels(tile_pixels)) return rc;
-    std::vector<patch_plan> plans;
-    if (int rc = plan_all(h_shapes, n_patches, tile_pixels, false, plans)) return rc;
-    return count_from(h_shapes, n_patches, plans, out);
+    const fp_tile_rule r = single_class(tile_pixels);
+    return fp_plan_count_rule(h_shapes, n_patches, &r, out);
 }
 
 extern "C" int fp_plan_fill(const fp_patch_shape *h_shapes, int n_patches, int tile_pixels,
                             fp_exposure_desc *h_expos, fp_tile *h_tiles, fp_band_desc *h_bands,
                             int32_t *h_order, int32_t *h_perm)
 {
-    if (!h_shapes || n_patches < 1) return fp_set_error(FP_ERR_ARGUMENT, "fp_plan_fill: bad arguments");
     if (int rc = check_tile_pixels(tile_pixels)) return rc;
+    const fp_tile_rule r = single_class(tile_pixels);
+    return fp_plan_fill_rule(h_shapes, n_patches, &r, h_expos, h_tiles, h_bands, h_order, h_perm);
+}
+
+extern "C" int fp_plan_fill_rule(const fp_patch_shape *h_shapes, int n_patches, const fp_tile_rule *rule,
+                                 fp_exposure_desc *h_expos, fp_tile *h_tiles, fp_band_desc *h_bands,
+                                 int32_t *h_order, int32_t *h_perm)
+{
+    if (!h_shapes || n_patches < 1) return fp_set_error(FP_ERR_ARGUMENT, "fp_plan_fill: bad arguments");
+    if (int rc = check_rule(rule)) return rc;
     if (!h_expos || !h_tiles || !h_bands || !h_order || !h_perm)
         return fp_set_error(FP_ERR_ARGUMENT, "fp_plan_fill: NULL output table");
     std::vector<patch_plan> plans;
-    if (int rc = plan_all(h_shapes, n_patches, tile_pixels, true, plans)) return rc;
+    if (int rc = plan_all(h_shapes, n_patches, *rule, true, plans)) return rc;
     fp_plan_sizes z;
     if (int rc = count_from(h_shapes, n_patches, plans, &z)) return rc;
 
@@ -292,7 +343,7 @@ extern "C" int fp_plan_fill(const fp_patch_shape *h_shapes, int n_patches, int t
                     t.expo = (int32_t)ie;
                     t.perm_start = (int32_t)q;
                     t.n_pix = n;
-                    t.pad = 0;
+                    t.tile_pixels = pl.tile_cls[kt];
                     t.bbox[0] = t.bbox[1] = t.bbox[2] = t.bbox[3] = 0.f;
                     work[(size_t)it] = (int64_t)n * ng;
                     poff += stride;

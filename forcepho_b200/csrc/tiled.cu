@@ -54,6 +54,18 @@ __device__ unsigned long long g_phase[8];
 
 static_assert(FP_RUN == 32, "the forward pass sums runs of one 32-Gaussian ballot word");
 
+// Compensated FP32 addition (Kahan): s - c tracks the exact running sum to
+// about one FP32 rounding, whatever the number of terms.  Used by the FP32 +
+// Kahan precision variant (FP_KAHAN); the normal build flushes FP32 runs into
+// FP64 instead.
+__device__ __forceinline__ void kahan_add(float &s, float &c, float x)
+{
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
 // A chunk's last group of v < 32 Gaussians is replicated min(8, 32 / v) times
 // across the warp's lanes in the adjoint, each replica taking every k-th pixel;
 // 8 replicas read 8 consecutive float4 (128 B) per step.
@@ -152,6 +164,260 @@ __global__ void bbox_kernel(const fp_patch *const *__restrict__ patches,
 }
 
 // ---------------------------------------------------------------------------
+// pixel records in plan order (after a change of the patches' pixel values)
+// ---------------------------------------------------------------------------
+// One warp per tile: the tile's (x, y, data, ierr) gathered through the plan's
+// pixel order into contiguous 16-byte records, which the tile kernel then
+// reads with one coalesced vector load per pixel and no index array; the tile
+// boxes are recomputed on the way.
+__global__ void pack_kernel(const fp_patch *const *__restrict__ patches,
+                            const fp_exposure_desc *__restrict__ expos, fp_tile *tiles,
+                            const int32_t *__restrict__ perm, float4 *__restrict__ pix, int64_t n_tiles)
+{
+    const int64_t t = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    if (t >= n_tiles) return;
+    const int lane = threadIdx.x & 31;
+    const fp_tile tl = tiles[t];
+    const fp_patch *pt = patches[expos[tl.expo].patch];
+    float x0 = INFINITY, x1 = -INFINITY, y0 = INFINITY, y1 = -INFINITY;
+    for (int i = lane; i < tl.n_pix; i += 32) {
+        const int32_t ix = perm[tl.perm_start + i];
+        const float x = pt->xpix[ix], y = pt->ypix[ix];
+        pix[tl.perm_start + i] = make_float4(x, y, pt->data[ix], pt->ierr[ix]);
+        x0 = fminf(x0, x); x1 = fmaxf(x1, x);
+        y0 = fminf(y0, y); y1 = fmaxf(y1, y);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        x0 = fminf(x0, __shfl_xor_sync(0xffffffffu, x0, o));
+        x1 = fmaxf(x1, __shfl_xor_sync(0xffffffffu, x1, o));
+        y0 = fminf(y0, __shfl_xor_sync(0xffffffffu, y0, o));
+        y1 = fmaxf(y1, __shfl_xor_sync(0xffffffffu, y1, o));
+    }
+    if (lane == 0) {
+        tiles[t].bbox[0] = x0; tiles[t].bbox[1] = x1;
+        tiles[t].bbox[2] = y0; tiles[t].bbox[3] = y1;
+    }
+}
+
+// Forward pass of one tile, P pixels per thread (the tile holds at most
+// 256 P pixels): the model of each pixel over the tile's kept Gaussians, the
+// residual (written out when the patch has a residual array), the chi2 terms
+// reduced into s_red[FP_WARPS], and the nonzero-weight pixels (x, y, w) compacted
+// into s_pix in ascending order.  Returns their count (the same on every thread).
+template <int P>
+__device__ __forceinline__ int forward_tile(const fp_tile &tl, const fp_exposure_desc &ed, const fp_patch *pt,
+                                            const int32_t *__restrict__ perm, const float4 *__restrict__ pix,
+                                            const float4 *__restrict__ gfwd, const float4 *__restrict__ gbox,
+                                            const bool nocull, const int gc, const uint16_t *s_idx, float4 *s_ga,
+                                            float4 *s_gb, float4 *s_gbox, float4 *s_pix, int *s_int, double *s_red)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int npix = tl.n_pix;
+
+    // the tile's pixels are listed in the plan's pixel order (compact cells)
+    const int j0 = tid * P;
+    const int nval = npix - j0;
+    const int32_t *tperm = perm + tl.perm_start + j0;
+    int idx[P];
+    float xs[P], ys[P], ds[P], es[P];
+    if (pix != nullptr) {
+        // contiguous (x, y, data, ierr) records in plan order: one 16-byte
+        // load per pixel; the patch index only where a residual is written
+        const float4 *rec = pix + tl.perm_start + j0;
+        const bool want_idx = pt->residual != nullptr;
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            const float4 r = (k < nval) ? __ldg(rec + k) : make_float4(0.f, 0.f, 0.f, 0.f);
+            xs[k] = r.x; ys[k] = r.y; ds[k] = r.z; es[k] = r.w;
+            idx[k] = (k < nval && want_idx) ? __ldg(tperm + k) : -1;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < P; ++k) {
+            idx[k] = (k < nval) ? __ldg(tperm + k) : -1;
+            const bool ok = idx[k] >= 0;
+            xs[k] = ok ? __ldg(pt->xpix + idx[k]) : 0.f;
+            ys[k] = ok ? __ldg(pt->ypix + idx[k]) : 0.f;
+            ds[k] = ok ? __ldg(pt->data + idx[k]) : 0.f;
+            es[k] = ok ? __ldg(pt->ierr + idx[k]) : 0.f;
+        }
+    }
+    // this warp's pixel box: Gaussians whose box misses it are skipped by
+    // the whole warp (they have E > MAX_EXP_ARG at all of its pixels)
+    float wx0 = INFINITY, wx1 = -INFINITY, wy0 = INFINITY, wy1 = -INFINITY;
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        if (k < nval) {
+            wx0 = fminf(wx0, xs[k]); wx1 = fmaxf(wx1, xs[k]);
+            wy0 = fminf(wy0, ys[k]); wy1 = fmaxf(wy1, ys[k]);
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        wx0 = fminf(wx0, __shfl_xor_sync(0xffffffffu, wx0, o));
+        wx1 = fmaxf(wx1, __shfl_xor_sync(0xffffffffu, wx1, o));
+        wy0 = fminf(wy0, __shfl_xor_sync(0xffffffffu, wy0, o));
+        wy1 = fmaxf(wy1, __shfl_xor_sync(0xffffffffu, wy1, o));
+    }
+    if (nocull) { wx0 = wy0 = -INFINITY; wx1 = wy1 = INFINITY; }
+    // one row: every thread's pixels share their y (cell rows in row order),
+    // so the y-dependent products of a Gaussian are formed once per thread
+    bool same_y = true;
+#pragma unroll
+    for (int k = 1; k < P; ++k) same_y = same_y && (k >= nval || ys[k] == ys[0]);
+    const bool rowwise = __all_sync(0xffffffffu, same_y);
+#ifdef FP_KAHAN
+    float KS[P], KC[P];     // per-pixel compensated FP32 model sums
+#pragma unroll
+    for (int k = 0; k < P; ++k) KS[k] = KC[k] = 0.f;
+#else
+    double M[P];
+#pragma unroll
+    for (int k = 0; k < P; ++k) M[k] = 0.0;
+#endif
+
+    for (int c0 = 0; c0 < gc; c0 += FP_CHUNK) {
+        const int cn = min(FP_CHUNK, gc - c0);
+        __syncthreads();
+        for (int i = tid; i < cn; i += FP_THREADS) {
+            const int64_t gi = ed.gauss_offset + s_idx[c0 + i];
+            s_ga[i] = gfwd[2 * gi];
+            s_gb[i] = gfwd[2 * gi + 1];
+            s_gbox[i] = gbox[gi];
+        }
+        __syncthreads();
+        {
+            // runs of 32 Gaussians: lane l tests Gaussian r0 + l against the
+            // warp's pixel box, and the warp visits the hits of the run in
+            // ascending order; each run is summed in FP32, then added in FP64.
+            // Every lane takes part in the ballot, including lanes without
+            // pixels (their sums are never used).
+            for (int r0 = 0; r0 < cn; r0 += 32) {
+                const int il = r0 + lane;
+                bool hit = false;
+                if (il < cn) {
+                    const float4 bx = s_gbox[il];
+                    hit = !(bx.y < wx0 || bx.x > wx1 || bx.w < wy0 || bx.z > wy1);
+                }
+                unsigned word = __ballot_sync(0xffffffffu, hit);
+                float m[P];
+#pragma unroll
+                for (int k = 0; k < P; ++k) m[k] = 0.f;
+                if (rowwise) {
+                    while (word) {
+                        const int i = r0 + __ffs(word) - 1;
+                        word &= word - 1u;
+                        const float4 A = s_ga[i], B = s_gb[i];
+                        const float dy = ys[0] - A.y;
+                        const float ty = A.w * dy, uy = B.x * dy;     // c Fxy dy, c Fyy dy
+#pragma unroll
+                        for (int k = 0; k < P; ++k) {
+                            const float dx = xs[k] - A.x;
+                            const float vx = fmaf(A.z, dx, ty);
+                            const float vy = fmaf(A.w, dx, uy);
+                            const float e = fmaf(dy, vy, dx * vx);
+                            const float g = fp_ex2(e);
+                            const float h = fmaf(B.z, fmaf(vx, vx, vy * vy), B.y);
+#ifdef FP_KAHAN
+                            kahan_add(KS[k], KC[k], (e < FP_CUT_SCALED) ? 0.f : g * h);
+#else
+                            m[k] = (e < FP_CUT_SCALED) ? m[k] : fmaf(g, h, m[k]);
+#endif
+                        }
+                    }
+                } else {
+                    while (word) {
+                        const int i = r0 + __ffs(word) - 1;
+                        word &= word - 1u;
+                        const float4 A = s_ga[i], B = s_gb[i];
+#pragma unroll
+                        for (int k = 0; k < P; ++k) {
+                            const float dx = xs[k] - A.x, dy = ys[k] - A.y;
+                            const float vx = fmaf(A.z, dx, A.w * dy);
+                            const float vy = fmaf(B.x, dy, A.w * dx);
+                            const float e = fmaf(dy, vy, dx * vx);
+                            const float g = fp_ex2(e);
+                            const float h = fmaf(B.z, fmaf(vx, vx, vy * vy), B.y);
+#ifdef FP_KAHAN
+                            kahan_add(KS[k], KC[k], (e < FP_CUT_SCALED) ? 0.f : g * h);
+#else
+                            m[k] = (e < FP_CUT_SCALED) ? m[k] : fmaf(g, h, m[k]);
+#endif
+                        }
+                    }
+                }
+#ifndef FP_KAHAN
+#pragma unroll
+                for (int k = 0; k < P; ++k) M[k] += (double)m[k];
+#endif
+            }
+        }
+    }
+
+    // residual, chi2 term (f64, the reference's (r^2 - d^2) ierr^2 form), weight
+    float rs[P], ws[P];
+    double chi = 0.0;
+    int nz = 0;
+#ifdef FP_KAHAN
+    float chi_s = 0.f, chi_c = 0.f;     // this thread's chi2 terms, compensated FP32
+#endif
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+        const bool live = k < nval;
+#ifdef FP_KAHAN
+        const float r = ds[k] - (KS[k] - KC[k]);
+        rs[k] = r;
+        const float rif = r * es[k], dif = ds[k] * es[k];
+        kahan_add(chi_s, chi_c, live ? (rif - dif) * (rif + dif) : 0.f);
+        if (k == P - 1) chi = (double)chi_s - (double)chi_c;
+#else
+        const double rd = (double)ds[k] - M[k];
+        const float r = (float)rd;
+        rs[k] = r;
+        // chi2 term (r ierr - d ierr)(r ierr + d ierr) from the FP64 residual
+        const double rid = rd * (double)es[k], did = (double)ds[k] * (double)es[k];
+        chi += live ? (rid - did) * (rid + did) : 0.0;
+#endif
+        ws[k] = live ? -2.f * ((r * es[k]) * es[k]) : 0.f;
+        nz += (ws[k] != 0.f) ? 1 : 0;
+    }
+    if (pt->residual != nullptr) {
+#pragma unroll
+        for (int k = 0; k < P; ++k)
+            if (idx[k] >= 0) pt->residual[idx[k]] = rs[k];
+    }
+
+    // compact nonzero-weight pixels (ascending) into s_pix; reduce chi2 (fixed tree)
+    int incl = nz;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) chi += __shfl_down_sync(0xffffffffu, chi, o);
+    if (lane == 31) s_int[8 + warp] = incl;
+    if (lane == 0) s_red[warp] = chi;
+    __syncthreads();
+    int off = incl - nz, nzt = 0;
+#pragma unroll
+    for (int w = 0; w < FP_WARPS; ++w) {
+        const int cnt = s_int[8 + w];
+        off += (w < warp) ? cnt : 0;
+        nzt += cnt;
+    }
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        if (ws[k] != 0.f) s_pix[off++] = make_float4(xs[k], ys[k], ws[k], 0.f);
+    if (tid == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < FP_WARPS; ++w) t += s_red[w];
+        s_red[FP_WARPS] = t;
+    }
+    return nzt;
+}
+
+// ---------------------------------------------------------------------------
 // tile kernel helpers
 // ---------------------------------------------------------------------------
 // Adjoint moments of one Gaussian (params A, B) over pixels p0, p0 + k, ... < p1
@@ -159,6 +425,49 @@ __global__ void bbox_kernel(const fp_patch *const *__restrict__ patches,
 // the cutoff), H the pixel-integral factor and v' = c F dx:
 //   m0 K, m1 KH, m2 KH vx', m3 KH vy', m4 K vx', m5 K vy', m6 KH dx^2,
 //   m7 KH dy^2, m8 KH dx dy, m9 K dx vx', m10 K dy vy', m11 K (dx vy' + dy vx')
+#ifdef FP_KAHAN
+// The FP32 + Kahan variant of the moments below (diagnostic build
+// libforcepho_b200_kahan.so): every moment summed over the whole pixel range
+// in FP32 with a compensation term, converted to FP64 once at the end.
+template <bool STRIDED>
+__device__ __forceinline__ void adjoint_moments(const float4 A, const float4 B,
+                                                const float4 *__restrict__ s_pix, int p0, int p1, int k,
+                                                double (&m)[12])
+{
+    const float xc = A.x, yc = A.y, fxs = A.z, fxys = A.w, fys = B.x, k0 = B.w;
+    const float c24 = (float)FP_C24;
+    const int step = STRIDED ? k : 1;
+    float a[12], c[12];
+#pragma unroll
+    for (int j = 0; j < 12; ++j) a[j] = c[j] = 0.f;
+    for (int p = p0; p < p1; p += step) {
+        const float4 q = s_pix[p];
+        const float dx = q.x - xc, dy = q.y - yc;
+        const float vx = fmaf(fxs, dx, fxys * dy);
+        const float vy = fmaf(fys, dy, fxys * dx);
+        const float pp = dx * vx;
+        const float e = fmaf(dy, vy, pp);
+        const float g = fp_ex2(e);
+        const float K = (e < FP_CUT_SCALED) ? 0.f : q.z * g;
+        const float s2 = fmaf(vx, vx, vy * vy);
+        const float KH = K * fmaf(s2, c24, k0);
+        kahan_add(a[0], c[0], K);
+        kahan_add(a[1], c[1], KH);
+        kahan_add(a[2], c[2], KH * vx);
+        kahan_add(a[3], c[3], KH * vy);
+        kahan_add(a[4], c[4], K * vx);
+        kahan_add(a[5], c[5], K * vy);
+        kahan_add(a[6], c[6], KH * dx * dx);
+        kahan_add(a[7], c[7], KH * dy * dy);
+        kahan_add(a[8], c[8], KH * dx * dy);
+        kahan_add(a[9], c[9], K * pp);
+        kahan_add(a[10], c[10], K * (e - pp));
+        kahan_add(a[11], c[11], K * fmaf(dx, vy, dy * vx));
+    }
+#pragma unroll
+    for (int j = 0; j < 12; ++j) m[j] += (double)a[j] - (double)c[j];
+}
+#else
 template <bool STRIDED>
 __device__ __forceinline__ void adjoint_moments(const float4 A, const float4 B,
                                                 const float4 *__restrict__ s_pix, int p0, int p1, int k,
@@ -201,6 +510,7 @@ __device__ __forceinline__ void adjoint_moments(const float4 A, const float4 B,
         m[6] += a6; m[7] += a7; m[8] += a8; m[9] += a9; m[10] += a10; m[11] += a11;
     }
 }
+#endif
 
 // Image-space partials from the moments (the reference's dC/d{A,x,y,Fxx,Fyy,Fxy}
 // summed over pixels, common_kernel.cc:118-132), then the Jacobian to the 7
@@ -282,11 +592,13 @@ __host__ __device__ inline tile_smem tile_smem_layout(int tile_pixels, int max_g
 // ---------------------------------------------------------------------------
 // tile kernel
 // ---------------------------------------------------------------------------
+// P: pixels per thread of the plan's largest tile class (shared memory holds
+// 256 P pixels); each tile runs the forward pass of its own class.
 template <int P>
 __global__ void __launch_bounds__(FP_THREADS, 4)
 tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc *__restrict__ expos,
             const fp_tile *__restrict__ tiles, const int32_t *__restrict__ order,
-            const int32_t *__restrict__ perm, int64_t n_tiles,
+            const int32_t *__restrict__ perm, const float4 *__restrict__ pix, int64_t n_tiles,
             const float4 *__restrict__ gfwd, const float4 *__restrict__ gbox,
             const double *__restrict__ gjac, double *__restrict__ partials, fp_control *ctl,
             int max_gauss, int flags)
@@ -328,8 +640,12 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
         const int ng = ed.n_gauss, ns = ed.n_sources, n_psf = ed.n_psf;
         const int npix = tl.n_pix;
         double *out = partials + tl.partial_offset;
-        if (npix > T || ng > max_gauss || ns > MAXSOURCES) {
-            if (tid == 0) atomicOr(&ctl->status, npix > T ? FP_STATUS_TILE_SIZE : FP_STATUS_GAUSS_COUNT);
+        const int tp = tl.tile_pixels;
+        const bool bad_tile = npix > tp || tp > T || (tp != 256 && tp != 512 && tp != 1024);
+        if (bad_tile || ng > max_gauss || ns > MAXSOURCES) {
+            if (tid == 0)
+                atomicOr(&ctl->status, bad_tile ? FP_STATUS_TILE_SIZE
+                                                : (ng > max_gauss ? FP_STATUS_GAUSS_COUNT : FP_STATUS_SOURCES));
             for (int t = tid; t < 1 + ns * NPARAMS && t < 1 + MAXSOURCES * NPARAMS; t += FP_THREADS)
                 out[t] = 0.0;
             __syncthreads();
@@ -380,167 +696,17 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
         __syncthreads();
 
         FP_PHASE_MARK(ph1);
-        // ---- 2. forward: model of P pixels per thread ----
-        // the tile's pixels are listed in the plan's pixel order (compact cells)
-        const int j0 = tid * P;
-        const int nval = npix - j0;
-        const int32_t *tperm = perm + tl.perm_start + j0;
-        int idx[P];
-        float xs[P], ys[P], ds[P], es[P];
-#pragma unroll
-        for (int k = 0; k < P; ++k) {
-            idx[k] = (k < nval) ? __ldg(tperm + k) : -1;
-            const bool ok = idx[k] >= 0;
-            xs[k] = ok ? __ldg(pt->xpix + idx[k]) : 0.f;
-            ys[k] = ok ? __ldg(pt->ypix + idx[k]) : 0.f;
-            ds[k] = ok ? __ldg(pt->data + idx[k]) : 0.f;
-            es[k] = ok ? __ldg(pt->ierr + idx[k]) : 0.f;
-        }
-        // this warp's pixel box: Gaussians whose box misses it are skipped by
-        // the whole warp (they have E > MAX_EXP_ARG at all of its pixels)
-        float wx0 = INFINITY, wx1 = -INFINITY, wy0 = INFINITY, wy1 = -INFINITY;
-#pragma unroll
-        for (int k = 0; k < P; ++k)
-            if (k < nval) {
-                wx0 = fminf(wx0, xs[k]); wx1 = fmaxf(wx1, xs[k]);
-                wy0 = fminf(wy0, ys[k]); wy1 = fmaxf(wy1, ys[k]);
-            }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            wx0 = fminf(wx0, __shfl_xor_sync(0xffffffffu, wx0, o));
-            wx1 = fmaxf(wx1, __shfl_xor_sync(0xffffffffu, wx1, o));
-            wy0 = fminf(wy0, __shfl_xor_sync(0xffffffffu, wy0, o));
-            wy1 = fmaxf(wy1, __shfl_xor_sync(0xffffffffu, wy1, o));
-        }
-        if (nocull) { wx0 = wy0 = -INFINITY; wx1 = wy1 = INFINITY; }
-        // one row: every thread's pixels share their y (cell rows in row order),
-        // so the y-dependent products of a Gaussian are formed once per thread
-        bool same_y = true;
-#pragma unroll
-        for (int k = 1; k < P; ++k) same_y = same_y && (k >= nval || ys[k] == ys[0]);
-        const bool rowwise = __all_sync(0xffffffffu, same_y);
-        double M[P];
-#pragma unroll
-        for (int k = 0; k < P; ++k) M[k] = 0.0;
-
-        for (int c0 = 0; c0 < gc; c0 += FP_CHUNK) {
-            const int cn = min(FP_CHUNK, gc - c0);
-            __syncthreads();
-            for (int i = tid; i < cn; i += FP_THREADS) {
-                const int64_t gi = ed.gauss_offset + s_idx[c0 + i];
-                s_ga[i] = gfwd[2 * gi];
-                s_gb[i] = gfwd[2 * gi + 1];
-                s_gbox[i] = gbox[gi];
-            }
-            __syncthreads();
-            {
-                // runs of 32 Gaussians: lane l tests Gaussian r0 + l against the
-                // warp's pixel box, and the warp visits the hits of the run in
-                // ascending order; each run is summed in FP32, then added in FP64.
-                // Every lane takes part in the ballot, including lanes without
-                // pixels (their sums are never used).
-                for (int r0 = 0; r0 < cn; r0 += 32) {
-                    const int il = r0 + lane;
-                    bool hit = false;
-                    if (il < cn) {
-                        const float4 bx = s_gbox[il];
-                        hit = !(bx.y < wx0 || bx.x > wx1 || bx.w < wy0 || bx.z > wy1);
-                    }
-                    unsigned word = __ballot_sync(0xffffffffu, hit);
-                    float m[P];
-#pragma unroll
-                    for (int k = 0; k < P; ++k) m[k] = 0.f;
-                    if (rowwise) {
-                        while (word) {
-                            const int i = r0 + __ffs(word) - 1;
-                            word &= word - 1u;
-                            const float4 A = s_ga[i], B = s_gb[i];
-                            const float dy = ys[0] - A.y;
-                            const float ty = A.w * dy, uy = B.x * dy;     // c Fxy dy, c Fyy dy
-#pragma unroll
-                            for (int k = 0; k < P; ++k) {
-                                const float dx = xs[k] - A.x;
-                                const float vx = fmaf(A.z, dx, ty);
-                                const float vy = fmaf(A.w, dx, uy);
-                                const float e = fmaf(dy, vy, dx * vx);
-                                const float g = fp_ex2(e);
-                                const float h = fmaf(B.z, fmaf(vx, vx, vy * vy), B.y);
-                                m[k] = (e < FP_CUT_SCALED) ? m[k] : fmaf(g, h, m[k]);
-                            }
-                        }
-                    } else {
-                        while (word) {
-                            const int i = r0 + __ffs(word) - 1;
-                            word &= word - 1u;
-                            const float4 A = s_ga[i], B = s_gb[i];
-#pragma unroll
-                            for (int k = 0; k < P; ++k) {
-                                const float dx = xs[k] - A.x, dy = ys[k] - A.y;
-                                const float vx = fmaf(A.z, dx, A.w * dy);
-                                const float vy = fmaf(B.x, dy, A.w * dx);
-                                const float e = fmaf(dy, vy, dx * vx);
-                                const float g = fp_ex2(e);
-                                const float h = fmaf(B.z, fmaf(vx, vx, vy * vy), B.y);
-                                m[k] = (e < FP_CUT_SCALED) ? m[k] : fmaf(g, h, m[k]);
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int k = 0; k < P; ++k) M[k] += (double)m[k];
-                }
-            }
-        }
-
-        // residual, chi2 term (f64, the reference's (r^2 - d^2) ierr^2 form), weight
-        float rs[P], ws[P];
-        double chi = 0.0;
-        int nz = 0;
-#pragma unroll
-        for (int k = 0; k < P; ++k) {
-            const bool live = k < nval;
-            const double rd = (double)ds[k] - M[k];
-            const float r = (float)rd;
-            rs[k] = r;
-            // chi2 term (r ierr - d ierr)(r ierr + d ierr) from the FP64 residual
-            const double rid = rd * (double)es[k], did = (double)ds[k] * (double)es[k];
-            chi += live ? (rid - did) * (rid + did) : 0.0;
-            ws[k] = live ? -2.f * ((r * es[k]) * es[k]) : 0.f;
-            nz += (ws[k] != 0.f) ? 1 : 0;
-        }
-        if (pt->residual != nullptr) {
-#pragma unroll
-            for (int k = 0; k < P; ++k)
-                if (idx[k] >= 0) pt->residual[idx[k]] = rs[k];
-        }
-
-        // compact nonzero-weight pixels (ascending) into s_pix; reduce chi2 (fixed tree)
-        int incl = nz;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) chi += __shfl_down_sync(0xffffffffu, chi, o);
-        if (lane == 31) s_int[8 + warp] = incl;
-        if (lane == 0) s_red[warp] = chi;
-        __syncthreads();
-        int off = incl - nz, nzt = 0;
-#pragma unroll
-        for (int w = 0; w < FP_WARPS; ++w) {
-            const int cnt = s_int[8 + w];
-            off += (w < warp) ? cnt : 0;
-            nzt += cnt;
-        }
-#pragma unroll
-        for (int k = 0; k < P; ++k)
-            if (ws[k] != 0.f) s_pix[off++] = make_float4(xs[k], ys[k], ws[k], 0.f);
-        if (tid == 0) {
-            double t = 0.0;
-#pragma unroll
-            for (int w = 0; w < FP_WARPS; ++w) t += s_red[w];
-            s_red[FP_WARPS] = t;
-        }
+        // ---- 2. forward: the tile's pixel class sets the pixels per thread ----
+        int nzt;
+        if (tl.tile_pixels == 1024)
+            nzt = forward_tile<4>(tl, ed, pt, perm, pix, gfwd, gbox, nocull, gc, s_idx, s_ga, s_gb, s_gbox, s_pix,
+                                  s_int, s_red);
+        else if (tl.tile_pixels == 512)
+            nzt = forward_tile<2>(tl, ed, pt, perm, pix, gfwd, gbox, nocull, gc, s_idx, s_ga, s_gb, s_gbox, s_pix,
+                                  s_int, s_red);
+        else
+            nzt = forward_tile<1>(tl, ed, pt, perm, pix, gfwd, gbox, nocull, gc, s_idx, s_ga, s_gb, s_gbox, s_pix,
+                                  s_int, s_red);
         for (int t = tid; t < FP_WARPS * MAXSOURCES * NPARAMS; t += FP_THREADS) s_wsrc[t] = 0.0;
 
         FP_PHASE_MARK(ph2);
@@ -772,7 +938,8 @@ int launch_tiles(int grid, size_t smem, cudaStream_t st, const fp_patch *const *
             return rc;
         if (dev >= 0 && dev < ATTR_MAX_DEVICES) g_attr_set[dev][pi].store(true);
     }
-    tile_kernel<P><<<grid, FP_THREADS, smem, st>>>(d_patches, tb.expos, tb.tiles, tb.order, tb.perm, n_tiles,
+    tile_kernel<P><<<grid, FP_THREADS, smem, st>>>(d_patches, tb.expos, tb.tiles, tb.order, tb.perm,
+                                                    reinterpret_cast<const float4 *>(tb.pix), n_tiles,
                                                     gfwd, gbox, gjac, partials, ctl, max_gauss, flags);
     return fp_check_cuda(cudaGetLastError(), "tile_kernel launch");
 }
@@ -797,6 +964,21 @@ extern "C" int fp_plan_bbox(const fp_patch *const *d_patches, const fp_plan_size
     bbox_kernel<<<(unsigned)grid, 32 * per_block, 0, (cudaStream_t)stream>>>(d_patches, tables->expos, tables->tiles,
                                                                           tables->perm, sizes->n_tiles);
     return fp_check_cuda(cudaGetLastError(), "bbox_kernel launch");
+}
+
+extern "C" int fp_plan_pack(const fp_patch *const *d_patches, const fp_plan_sizes *sizes,
+                            const fp_plan_tables *tables, float *d_pix, void *stream)
+{
+    if (!d_patches || !sizes || sizes->n_tiles < 0 || !d_pix)
+        return fp_set_error(FP_ERR_ARGUMENT, "fp_plan_pack: bad arguments");
+    if (((uintptr_t)d_pix) & 15) return fp_set_error(FP_ERR_ARGUMENT, "fp_plan_pack: records must be 16-byte aligned");
+    if (int rc = check_tables(tables, "fp_plan_pack")) return rc;
+    if (sizes->n_tiles == 0) return FP_OK;
+    const int per_block = 8;
+    const int64_t grid = (sizes->n_tiles + per_block - 1) / per_block;
+    pack_kernel<<<(unsigned)grid, 32 * per_block, 0, (cudaStream_t)stream>>>(
+        d_patches, tables->expos, tables->tiles, tables->perm, reinterpret_cast<float4 *>(d_pix), sizes->n_tiles);
+    return fp_check_cuda(cudaGetLastError(), "pack_kernel launch");
 }
 
 extern "C" int fp_tile_smem_bytes(int tile_pixels, int64_t max_gauss, int64_t *out)
@@ -851,6 +1033,7 @@ int check_batch(const fp_patch *const *d_patches, int n_patches, const fp_plan_s
     if (!d_patches || n_patches < 1 || !sizes || !d_proposals || !d_chi2 || !d_response || !launch)
         return fp_set_error(FP_ERR_ARGUMENT, "%s: NULL argument", who);
     if (int rc = check_tables(tables, who)) return rc;
+    if (((uintptr_t)tables->pix) & 15) return fp_set_error(FP_ERR_ARGUMENT, "%s: pixel records must be 16-byte aligned", who);
     const fp_workspace_layout L = fp_layout(sizes->n_gauss, sizes->n_partials);
     if (workspace_bytes < L.total)
         return fp_set_error(FP_ERR_WORKSPACE, "%s: workspace %zu B < required %zu B", who, workspace_bytes,

@@ -110,6 +110,7 @@ class B200PatchMixin:
         self.send_patchstruct_to_device()
         self._dirty_data = False
         self.device_generation = next(_UPLOADS)
+        self.data_generation = next(_UPLOADS)
         return self.device_patch
 
     def _alloc_residual(self):
@@ -146,6 +147,7 @@ class B200PatchMixin:
         d["data"], d["residual"] = d["residual"], d["data"]
         self.send_patchstruct_to_device()
         self._dirty_data = True
+        self.data_generation = next(_UPLOADS)     # plans re-pack their pixel records
         return self.device_patch
 
     def retrieve_array(self, arrname="residual"):
@@ -194,28 +196,33 @@ class Plan:
     the output buffers ``chi2`` f64[n_patches, MAXBANDS] and ``response``
     f32[n_patches, MAXBANDS, MAXSOURCES*NPARAMS]."""
 
-    def __init__(self, patches, tile_pixels=1024, device=None, stream=None, compact_tiles=True):
+    def __init__(self, patches, tile_pixels=1024, device=None, stream=None, compact_tiles=True, tile_classes=None):
         self.L = N.load()
         self.patches = list(patches)
         self.n = len(self.patches)
-        self.tile_pixels = int(tile_pixels)
+        # one tile size for every exposure, or per exposure-size class:
+        # tile_classes = [(max_exposure_pixels, tile_pixels), ...] (the last takes the rest)
+        self.tile_classes = None if tile_classes is None else [(int(a), int(b)) for a, b in tile_classes]
+        rule = N.tile_rule(self.tile_classes or [(2 ** 31 - 1, int(tile_pixels))])
+        self.rule = rule
+        self.tile_pixels = max(rule.tile_pixels[c] for c in range(rule.n_classes))
         dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.device = dev
         shapes = [N.patch_shape(p, coordinates=compact_tiles) for p in self.patches]
         self._shapes = (N.PatchShape * self.n)(*shapes)
         self._shape_keep = shapes
         sz = N.PlanSizes()
-        N.check(self.L.fp_plan_count(ctypes.addressof(self._shapes), self.n, self.tile_pixels, ctypes.byref(sz)),
-                "fp_plan_count")
+        N.check(self.L.fp_plan_count_rule(ctypes.addressof(self._shapes), self.n, ctypes.byref(rule),
+                                          ctypes.byref(sz)), "fp_plan_count_rule")
         self.sizes = sz
         h_expos = np.zeros(sz.n_exposures, dtype=N.exposure_desc_dtype)
         h_tiles = np.zeros(sz.n_tiles, dtype=N.tile_dtype)
         h_bands = np.zeros(sz.n_band_outputs, dtype=N.band_desc_dtype)
         h_order = np.zeros(sz.n_tiles, dtype=np.int32)
         h_perm = np.zeros(sz.n_perm, dtype=np.int32)
-        N.check(self.L.fp_plan_fill(ctypes.addressof(self._shapes), self.n, self.tile_pixels,
-                                    h_expos.ctypes.data, h_tiles.ctypes.data, h_bands.ctypes.data,
-                                    h_order.ctypes.data, h_perm.ctypes.data), "fp_plan_fill")
+        N.check(self.L.fp_plan_fill_rule(ctypes.addressof(self._shapes), self.n, ctypes.byref(rule),
+                                         h_expos.ctypes.data, h_tiles.ctypes.data, h_bands.ctypes.data,
+                                         h_order.ctypes.data, h_perm.ctypes.data), "fp_plan_fill_rule")
         self.h_expos, self.h_tiles, self.h_bands, self.h_order = h_expos, h_tiles, h_bands, h_order
         self.h_perm = h_perm
         self.d_expos = to_device_bytes(h_expos, dev)
@@ -223,29 +230,46 @@ class Plan:
         self.d_bands = to_device_bytes(h_bands, dev)
         self.d_order = to_device_bytes(h_order, dev)
         self.d_perm = to_device_bytes(h_perm, dev)
+        # (x, y, data, ierr) records of every tile pixel in plan order, read by
+        # the tile kernel as one 16-byte load per pixel (fp_plan_pack)
+        self.d_pix = torch.empty(max(int(sz.n_perm), 1) * 16, dtype=torch.uint8, device=dev)
         self.tables = N.PlanTables(_ptr(self.d_expos), _ptr(self.d_tiles), _ptr(self.d_order),
-                                   _ptr(self.d_bands), _ptr(self.d_perm))
+                                   _ptr(self.d_bands), _ptr(self.d_perm), _ptr(self.d_pix))
         self.d_patches = torch.zeros(self.n, dtype=torch.int64, device=dev)
         # what the tables were made from: each patch's upload and device struct
         # (holding the struct keeps its memory from being reused)
         self._stamps = [(getattr(p, "device_generation", None), p.device_patch) for p in self.patches]
         self.refresh_patch_pointers()
-        st = current_stream_ptr(stream)
-        N.check(self.L.fp_plan_bbox(_ptr(self.d_patches), ctypes.byref(sz), ctypes.byref(self.tables), st),
-                "fp_plan_bbox")
+        self._packed = None
+        self.pack(stream)
         self.workspace = torch.zeros(max(sz.workspace_bytes, 256), dtype=torch.uint8, device=dev)
         self.proposals = torch.zeros(self.n * MAXSOURCES * source_struct_dtype.itemsize, dtype=torch.uint8,
                                      device=dev)
         self.chi2 = torch.zeros((self.n, MAXBANDS), dtype=torch.float64, device=dev)
         self.response = torch.zeros((self.n, MAXBANDS, MAXSOURCES * NPARAMS), dtype=torch.float32, device=dev)
 
-    def check_current(self):
+    def _data_stamps(self):
+        return [getattr(p, "data_generation", None) for p in self.patches]
+
+    def pack(self, stream=None):
+        """Queue the gather of every tile pixel's (x, y, data, ierr) into the
+        plan's records (and the tile boxes) from the patches' current arrays."""
+        N.check(self.L.fp_plan_pack(_ptr(self.d_patches), ctypes.byref(self.sizes), ctypes.byref(self.tables),
+                                    _ptr(self.d_pix), current_stream_ptr(stream)), "fp_plan_pack")
+        self._packed = self._data_stamps()
+
+    def check_current(self, stream=None):
         """Raise if a patch was freed or sent to the device again since the plan
-        was made: its tiles, pixel order and boxes describe the old upload."""
+        was made: its tiles, pixel order and boxes describe the old upload.
+        Re-pack the pixel records (queued on ``stream``) if a patch's device
+        data changed since the last pack (``swap_on_device``).  Every
+        evaluation and graph replay of the plan is preceded by this call."""
         for i, (p, (gen, struct)) in enumerate(zip(self.patches, self._stamps)):
             if getattr(p, "device_generation", None) != gen or getattr(p, "device_patch", None) is not struct:
                 raise RuntimeError("patch %d was freed or sent to the device again after this plan was made; "
                                    "make a new plan (or proposer) for it" % i)
+        if self._data_stamps() != self._packed:
+            self.pack(stream)
 
     def refresh_patch_pointers(self):
         ptrs = torch.tensor([p.device_patch_ptr for p in self.patches], dtype=torch.int64)
@@ -271,7 +295,7 @@ class Plan:
         """Queue one evaluation of the proposals in ``self.proposals`` (or the
         given device buffer) on ``stream``; outputs land in ``self.chi2`` /
         ``self.response`` (or the given buffers).  No host synchronisation."""
-        self.check_current()
+        self.check_current(stream)
         lp = launch if launch is not None else self.launch()
         props = self.proposals if proposals is None else proposals
         c2 = self.chi2 if chi2 is None else chi2

@@ -13,8 +13,13 @@ Metropolis test.
 
 Fixed-length HMC with a diagonal mass matrix stands in for NUTS.  The mass
 matrix is estimated from the curvature of lnp at the start (Hutchinson probes
-of the Hessian diagonal with the analytic gradient), and the step size of each
-patch is adapted during warm-up trajectories towards a target acceptance rate.
+of the Hessian diagonal with the analytic gradient) and, optionally, from the
+variance of the warm-up draws.  The step size of each patch is adapted during
+warm-up trajectories by dual averaging (Hoffman & Gelman 2014, algorithm 5,
+as in Stan and in littlemcmc's NUTS) towards a target acceptance
+probability; after warm-up each patch keeps its averaged step size.  The
+adaptation runs as device tensor operations between graph replays, with no
+host synchronisation.
 """
 
 import ctypes
@@ -190,24 +195,70 @@ class DeviceHMC:
         self.graph = g
         return g
 
-    def run(self, n_traj, adapt=False, target=0.65):
-        """Run n_traj trajectories (graph replays).  With ``adapt`` the step
-        size of each patch follows the acceptance of each trajectory."""
+    def run(self, n_traj, adapt=False, target=0.8, record=None):
+        """Run n_traj trajectories (graph replays).
+
+        adapt : dual-averaging step-size adaptation of every patch towards a
+            mean acceptance probability ``target`` after each trajectory; the
+            averaged step size is installed by ``end_adaptation``.
+        record : optional {trajectory index within this call: device tensor}
+            that receives a copy of the positions z after that trajectory
+            (a device copy, no host synchronisation)."""
         self.plan.check_current()
         if self.graph is None:
             self.capture()
         if int(self.traj.item()) + n_traj > self.max_traj:
             raise ValueError("not enough pre-drawn random numbers (max_traj=%d)" % self.max_traj)
-        for _ in range(n_traj):
-            before = self.accepted.clone() if adapt else None
+        if adapt and getattr(self, "_da", None) is None:
+            self.start_adaptation(target)
+        for t in range(n_traj):
             self.graph.replay()
             self.n_evals += self.n_steps
             if adapt:
-                acc = (self.accepted - before).to(torch.float64)
-                prob = torch.clamp(torch.exp(torch.clamp(self.energy_error, max=0.0)), 0, 1)
-                stat = 0.5 * acc + 0.5 * prob
-                self.eps.mul_(torch.exp(0.6 * (stat - target)))
+                self._adapt_step()
+            if record is not None and t in record:
+                record[t].copy_(self.z)
         return self
+
+    # --- dual averaging of the step sizes (device tensors) ---
+    def start_adaptation(self, target=0.8, gamma=0.05, kappa=0.75, t0=10.0):
+        """Start (or restart) the dual averaging of every patch's step size from
+        the current step sizes (Hoffman & Gelman 2014, algorithm 5)."""
+        f64 = dict(dtype=torch.float64, device=self.device)
+        self._da = {"mu": torch.log(10.0 * self.eps), "hbar": torch.zeros(self.n, **f64),
+                    "log_bar": torch.zeros(self.n, **f64), "m": 0, "target": float(target),
+                    "gamma": gamma, "kappa": kappa, "t0": t0}
+
+    def _adapt_step(self):
+        d = self._da
+        d["m"] += 1
+        m = float(d["m"])
+        # acceptance probability of the trajectory just run: min(1, exp(H0 - H1))
+        ee = torch.nan_to_num(self.energy_error, nan=-1e30, posinf=-1e30, neginf=-1e30)
+        alpha = torch.exp(torch.clamp(ee, max=0.0))
+        eta = 1.0 / (m + d["t0"])
+        d["hbar"].mul_(1.0 - eta).add_(eta * (d["target"] - alpha))
+        log_eps = d["mu"] - (m ** 0.5 / d["gamma"]) * d["hbar"]
+        w = m ** (-d["kappa"])
+        d["log_bar"].mul_(1.0 - w).add_(w * log_eps)
+        self.eps.copy_(torch.exp(log_eps))
+
+    def end_adaptation(self):
+        """Install each patch's averaged step size and stop adapting."""
+        if getattr(self, "_da", None) is not None and self._da["m"] > 0:
+            self.eps.copy_(torch.exp(self._da["log_bar"]))
+        self._da = None
+
+    def adapt_mass_from(self, draws, reg=5.0):
+        """Diagonal inverse mass matrix from warm-up draws of z (device tensor
+        [n_draws, n_params]): the sample variance, shrunk towards 1e-3 as Stan
+        does ((n / (n + 5)) var + 1e-3 (5 / (n + 5)))."""
+        n = draws.shape[0]
+        if n < 2:
+            return self.inv_mass
+        var = draws.var(dim=0, unbiased=True)
+        self.inv_mass.copy_((n / (n + reg)) * var + 1e-3 * (reg / (n + reg)))
+        return self.inv_mass
 
     def estimate_inv_mass(self, n_probe=8, h=1e-3, floor=1e-8, seed=1):
         """inv_mass = 1 / diag(-d2 lnp / dz2), the Hessian diagonal estimated with

@@ -128,7 +128,7 @@ class B200Proposer(ProposerBase):
             if self._graph is None or self._graph_key != gkey:
                 self._capture(plan, lp, stream)
                 self._graph_key = gkey
-            plan.check_current()
+            plan.check_current(stream)
             self._graph.replay()
         else:
             self._queue(plan, lp)

@@ -15,6 +15,8 @@
  *     printed.  fp_error_string() gives a one-line description of the last error.
  *   - Entry points never allocate device memory: buffers are owned by the caller
  *     (the reference's Python patch objects own theirs, forcepho/patches/device_patch.py:265-297).
+ *     The one exception is fp_evaluate_proposal, the reference's own kernel ABI,
+ *     which keeps a library-owned work plan per patch (fp_evaluate_proposal_release).
  *   - Launches are asynchronous on `stream` and contain no host synchronisation, so a
  *     sequence of them can be captured into a CUDA graph.  The one exception is
  *     fp_evaluate_proposal, which reads the patch struct back before its launch.
@@ -162,16 +164,33 @@ FP_API int fp_evaluate_proposal_plain(const fp_patch *d_patch, const fp_source *
                                int n_bands, int max_gauss_per_exposure,
                                double *d_chi2, fp_response *d_response, void *stream);
 
-/* The same evaluation with the kernel ABI of the reference's
- * EvaluateProposal (forcepho/src/compute_gaussians_kernel.cu:212-214): device
- * patch, device sources, output chi2[n_bands] and Response[n_bands].  It sizes
- * shared memory from the patch itself, so it copies the 152-byte struct and
- * n_psf_per_source[n_bands] back to the host and waits for them on `stream`
- * before the launch (the result is still produced asynchronously on
- * `stream`).  n_sources must equal the struct's n_sources (FP_ERR_ARGUMENT
- * otherwise).  For many patches, or the tiled kernels, use fp_evaluate_batch. */
+/* One proposal on one patch with the kernel ABI of the reference's
+ * EvaluateProposal (forcepho/src/compute_gaussians_kernel.cu:212-214, launched
+ * by GPUProposer.evaluate_proposal, forcepho/proposal.py:96-152): device patch
+ * struct, device sources[n_sources], outputs chi2[n_bands] (f64) and
+ * Response[n_bands], evaluated by the tiled B200 kernels (the path of
+ * fp_evaluate_batch, not the plain comparator).
+ *
+ * The tiled kernels need a work plan of the patch.  The library keeps one per
+ * device patch struct (and device), made on first use from the patch's own
+ * device arrays and kept while the struct's xpix/ypix/index-array pointers,
+ * n_sources and the index arrays' contents stay the same; otherwise it is
+ * made anew.  Each call therefore reads the 152-byte struct and the index
+ * arrays back to the host (two waits on `stream`; a new plan adds one for the
+ * coordinates), then queues three launches that produce the results
+ * asynchronously on `stream`.  Tile bounding boxes are recomputed every call,
+ * so coordinates rewritten in place stay exact.  Plans (tables and workspace:
+ * about 216 B per image Gaussian plus 40 B per pixel tile) are device memory
+ * owned by the library, at most 64 of them (least recently used first out),
+ * until fp_evaluate_proposal_release.  Calls on one patch must not overlap on
+ * the GPU: they share its plan's workspace.  n_sources must equal the struct's
+ * n_sources (FP_ERR_ARGUMENT otherwise). */
 FP_API int fp_evaluate_proposal(const fp_patch *d_patch, const fp_source *d_sources, int n_sources,
                                 int n_bands, double *d_chi2, fp_response *d_response, void *stream);
+
+/* Free every plan fp_evaluate_proposal keeps (waits for the device first).
+ * No counterpart in the reference (its kernel keeps no state). */
+FP_API int fp_evaluate_proposal_release(void);
 
 /* ------------------------------------------------------------------------- */
 /* Tiled / batched path.                                                     */
@@ -216,7 +235,7 @@ typedef struct fp_tile {
     int32_t expo;           /* index into the plan's fp_exposure_desc table */
     int32_t perm_start;     /* first entry of this tile in the plan's pixel order */
     int32_t n_pix;          /* pixels in the tile (<= tile_pixels) */
-    int32_t pad;
+    int32_t tile_pixels;    /* the tile's size class (256, 512 or 1024): 1, 2 or 4 pixels per thread */
     float bbox[4];          /* xmin, xmax, ymin, ymax of the tile's pixels (device-filled) */
 } fp_tile;                 /* 40 bytes */
 
@@ -250,6 +269,9 @@ typedef struct fp_plan_tables {
     const int32_t *order;           /* [n_tiles] execution order, most work first */
     const fp_band_desc *bands;      /* [n_band_outputs] */
     const int32_t *perm;            /* [n_perm] index within its patch of every tile pixel, tile after tile */
+    const float *pix;               /* [n_perm][4] (x, y, data, ierr) of every tile pixel in the same order,
+                                       16-byte aligned (fp_plan_pack), or NULL: the tile kernel then reads
+                                       the patch arrays through perm */
 } fp_plan_tables;
 
 /* Count the plan of `n_patches` patches split into tiles of at most
@@ -260,6 +282,26 @@ typedef struct fp_plan_tables {
  * with more pixels than a tile is split. */
 FP_API int fp_plan_count(const fp_patch_shape *h_shapes, int n_patches, int tile_pixels,
                   fp_plan_sizes *out);
+
+/* Tile size by exposure size: a plan may hold tiles of several size classes,
+ * all evaluated in the same persistent launch.  An exposure of n pixels takes
+ * the first class c with n <= max_exposure_pixels[c] (the last class takes
+ * every larger one) and is split into tiles of tile_pixels[c] pixels (cells of
+ * the image plane as for fp_plan_count).  The kernels support 256, 512 and
+ * 1024; the launch's tile_pixels must be the largest class of the plan. */
+#define FP_MAX_TILE_CLASSES 4
+typedef struct fp_tile_rule {
+    int32_t n_classes;                               /* 1 .. FP_MAX_TILE_CLASSES */
+    int32_t max_exposure_pixels[FP_MAX_TILE_CLASSES];  /* ascending; ignored for the last class */
+    int32_t tile_pixels[FP_MAX_TILE_CLASSES];
+} fp_tile_rule;
+
+/* fp_plan_count and fp_plan_fill with a tile rule instead of one tile size. */
+FP_API int fp_plan_count_rule(const fp_patch_shape *h_shapes, int n_patches, const fp_tile_rule *rule,
+                              fp_plan_sizes *out);
+FP_API int fp_plan_fill_rule(const fp_patch_shape *h_shapes, int n_patches, const fp_tile_rule *rule,
+                             fp_exposure_desc *h_expos, fp_tile *h_tiles, fp_band_desc *h_bands,
+                             int32_t *h_order, int32_t *h_perm);
 
 /* Fill the host tables of a plan (sizes from fp_plan_count).  Tiles are emitted
  * in canonical order (patch, band, exposure, cell); h_order receives an
@@ -275,9 +317,20 @@ FP_API int fp_plan_fill(const fp_patch_shape *h_shapes, int n_patches, int tile_
 FP_API int fp_plan_bbox(const fp_patch *const *d_patches, const fp_plan_sizes *sizes,
                         const fp_plan_tables *tables, void *stream);
 
+/* Fill d_pix[n_perm][4] with the (x, y, data, ierr) records of every tile
+ * pixel in the plan's pixel order (gathered through tables->perm) and
+ * recompute the tile boxes.  With tables->pix = d_pix, fp_evaluate_batch then
+ * reads each pixel as one contiguous 16-byte record instead of four gathers
+ * through the index array.  The records are a copy: run this again whenever
+ * any patch's data, ierr, xpix or ypix values or pointers change (for example
+ * after a data/residual swap), before the next evaluation on that stream.
+ * No reference counterpart (the reference kernel reads the SoA arrays). */
+FP_API int fp_plan_pack(const fp_patch *const *d_patches, const fp_plan_sizes *sizes,
+                        const fp_plan_tables *tables, float *d_pix, void *stream);
+
 /* Launch parameters of the batched evaluation (chosen by the autotuner). */
 typedef struct fp_launch {
-    int32_t tile_pixels;    /* pixels per tile: 256, 512 or 1024; must equal the plan's */
+    int32_t tile_pixels;    /* pixels per tile: 256, 512 or 1024; the plan's largest tile class */
     int32_t ctas_per_sm;    /* persistent CTAs per SM (grid = ctas_per_sm * SM count) */
     int32_t flags;          /* FP_FLAG_* */
     int32_t phases;         /* FP_PHASE_* bits to run; 0 = all three */

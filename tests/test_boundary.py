@@ -179,3 +179,46 @@ def test_validate_rejects_inconsistent_patch():
     r.psfgauss["sersic_bin"][0] = 12
     with pytest.raises(ValueError):
         r.validate()
+
+
+def test_planner_tile_rule_classes():
+    """A tile rule gives each exposure the tile size of its pixel-count class;
+    each tile records its class, and every pixel appears exactly once."""
+    L = N.load()
+    patches = S.config_batched(seed=9, n_patches=8)
+    shapes = [N.patch_shape(p) for p in patches]
+    arr = (N.PatchShape * len(shapes))(*shapes)
+    classes = [(4096, 256), (16384, 512), (1 << 30, 1024)]
+    rule = N.tile_rule(classes)
+    sz = N.PlanSizes()
+    N.check(L.fp_plan_count_rule(ctypes.addressof(arr), len(shapes), ctypes.byref(rule), ctypes.byref(sz)), "count")
+    ex = np.zeros(sz.n_exposures, N.exposure_desc_dtype)
+    ti = np.zeros(sz.n_tiles, N.tile_dtype)
+    bd = np.zeros(sz.n_band_outputs, N.band_desc_dtype)
+    od = np.zeros(sz.n_tiles, np.int32)
+    pm = np.zeros(sz.n_perm, np.int32)
+    N.check(L.fp_plan_fill_rule(ctypes.addressof(arr), len(shapes), ctypes.byref(rule), ex.ctypes.data,
+                                ti.ctypes.data, bd.ctypes.data, od.ctypes.data, pm.ctypes.data), "fill")
+    seen_classes = set()
+    for t in ti:
+        e = ex[t["expo"]]
+        p = patches[e["patch"]]
+        n = int(p.exposure_N[e["exposure"]])
+        want = 256 if n <= 4096 else (512 if n <= 16384 else 1024)
+        assert t["tile_pixels"] == want and 0 < t["n_pix"] <= want
+        seen_classes.add(want)
+    assert seen_classes == {256, 512, 1024}
+    off = 0
+    for p in patches:
+        assert sorted(pm[off:off + p.npix].tolist()) == list(range(p.npix))
+        off += p.npix
+    # a single tile size is the one-class rule
+    sz1 = N.PlanSizes()
+    N.check(L.fp_plan_count(ctypes.addressof(arr), len(shapes), 512, ctypes.byref(sz1)), "count")
+    sz2 = N.PlanSizes()
+    N.check(L.fp_plan_count_rule(ctypes.addressof(arr), len(shapes), ctypes.byref(N.tile_rule([(0, 512)])),
+                                 ctypes.byref(sz2)), "count")
+    assert sz1.n_tiles == sz2.n_tiles and sz1.n_partials == sz2.n_partials
+    bad = N.tile_rule([(4096, 256), (16384, 500)])
+    assert L.fp_plan_count_rule(ctypes.addressof(arr), len(shapes), ctypes.byref(bad), ctypes.byref(sz)) \
+        == N.FP_ERR_ARGUMENT

@@ -193,3 +193,51 @@ def test_shuffled_pixels_and_plan_without_coordinates():
     assert chi2_err(chi2, c64, sc) < CHI2_F64
     assert chi2_raw_err(chi2, c64, band_scales(p, r64)) < CHI2_F64
     assert grad_err(dchi2, g64) < GRAD_F64
+
+
+def test_mixed_tile_classes_in_one_launch(batch):
+    """A plan whose exposures take tiles of 256, 512 and 1024 pixels by size
+    class runs in one persistent launch: every patch matches the FP64 oracle,
+    the census drops no within-cutoff pair, and the per-class autotuner returns
+    a valid class list."""
+    from forcepho_b200.batch import BatchedProposer
+    from forcepho_b200.autotune import Autotuner
+    props = _perturbed(batch, 5)
+    classes = [(1600, 256), (3000, 512), (2 ** 31 - 1, 1024)]
+    bp = BatchedProposer(batch, tile_classes=classes)
+    tps = set(int(t) for t in bp.plan.h_tiles["tile_pixels"])
+    assert tps == {256, 512, 1024}, tps
+    assert bp.launch.tile_pixels == 1024
+    res = bp.evaluate_proposals(props)
+    for p, prop, (chi2, dchi2) in zip(batch, props, res):
+        c64, g64, r64 = O.evaluate(p, prop, precision="f64", return_residual=True)
+        assert chi2_raw_err(chi2, c64, band_scales(p, r64)) < CHI2_F64
+        assert grad_err(dchi2, g64) < GRAD_F64
+    assert bp.count_pairs()[2] == 0
+    tuned = BatchedProposer(batch, autotune="classes", tuner=Autotuner(reps=1))
+    assert len(tuned.tile_classes) == 3
+    assert all(tp in (256, 512, 1024) for _, tp in tuned.tile_classes)
+    res2 = tuned.evaluate_proposals(props)
+    for (c1, _), (c2, _), p in zip(res, res2, batch):
+        assert np.max(np.abs(c1 - c2) / np.maximum(np.abs(c1), 1e-300)) < 2 * CHI2_F64 or p.n_pairs() == 0
+
+
+def test_swapped_data_is_repacked_before_the_next_replay():
+    """The plan's pixel records are a copy of the device data: after
+    swap_on_device the next graph replay of a proposer sees the new data."""
+    from forcepho_b200 import synthetic as S
+    from forcepho_b200.proposal import B200Proposer
+    p = S.config_multiband(seed=41, n_sources=3, n_bands=2, exp_per_band=1, size=40)
+    p.return_residual = True
+    p.send_to_device()
+    prop = _perturbed([p], 2)[0]
+    pr = B200Proposer()
+    chi2a, _, res = pr.evaluate_proposal(prop, patch=p, unpack=False)
+    p.swap_on_device()                          # device data <- this residual
+    chi2b, dchi2b, _ = pr.evaluate_proposal(prop, patch=p, unpack=False)
+    q = S.config_multiband(seed=41, n_sources=3, n_bands=2, exp_per_band=1, size=40)
+    q.data = res.astype(np.float32)
+    c64, g64, r64 = O.evaluate(q, prop, precision="f64", return_residual=True)
+    assert not np.allclose(chi2a, chi2b)
+    assert chi2_raw_err(chi2b, c64, band_scales(q, r64)) < CHI2_F64
+    assert grad_err(dchi2b, g64) < GRAD_F64
