@@ -11,7 +11,10 @@ Modules, with the reference counterparts they stand in for:
 * ``nuts``        -- ``BatchedNUTS``, ``run_nuts`` (``forcepho.fitting.run_lmc``)
 * ``render``      -- ``subtract_fixed``, ``design_matrix``, ``render`` (``device_patch.py``)
 * ``fitting``     -- ``optimize_one_band``, ``optimize_fluxes`` (``forcepho.fitting``)
-* ``autograd``    -- ``PatchChi2``, a ``torch.autograd.Function`` over the kernels
+* ``autograd``    -- ``BatchChi2`` / ``PatchChi2``: per-band chi2 of many / one patch as a
+                     device-resident ``torch.autograd.Function`` of the scene parameters
+* ``stores``      -- ``FITSPatch``, ``StorePatch``, ``PSFStore``, regions, and the FITS, TAN-WCS
+                     and HDF5 readers (``forcepho.patches.pixel_patch``, ``storage``, ``forcepho.region``)
 * ``distributed`` -- ``PatchFarm``: patches shared out over processes / GPUs
 * ``sources``, ``patch``, ``structs``, ``kernel_limits``, ``splines`` -- the data
   model (``forcepho.sources``, ``forcepho.patches.patch``, ``forcepho.kernel_limits``)
