@@ -66,6 +66,26 @@ __device__ __forceinline__ float fp_ex2(float x)
     return y;
 }
 
+// L2 policy for data read once per evaluation (the pixel records): evict
+// first, so the stream does not push the per-exposure Gaussian tables, which
+// every tile of the exposure re-reads, out of L2.
+__device__ __forceinline__ uint64_t fp_policy_evict_first()
+{
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+// 16-byte read-only load with an L2 cache policy.
+__device__ __forceinline__ float4 fp_ldg_policy(const float4 *p, uint64_t pol)
+{
+    float4 r;
+    asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+        : "l"(p), "l"(pol));
+    return r;
+}
+
 // 2x2 matrices as {m11, m12, m21, m22}
 template <typename R>
 struct fp_m22 {

@@ -225,9 +225,10 @@ __device__ __forceinline__ int forward_tile(const fp_tile &tl, const fp_exposure
         // load per pixel; the patch index only where a residual is written
         const float4 *rec = pix + tl.perm_start + j0;
         const bool want_idx = pt->residual != nullptr;
+        const uint64_t pol = fp_policy_evict_first();
 #pragma unroll
         for (int k = 0; k < P; ++k) {
-            const float4 r = (k < nval) ? __ldg(rec + k) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 r = (k < nval) ? fp_ldg_policy(rec + k, pol) : make_float4(0.f, 0.f, 0.f, 0.f);
             xs[k] = r.x; ys[k] = r.y; ds[k] = r.z; es[k] = r.w;
             idx[k] = (k < nval && want_idx) ? __ldg(tperm + k) : -1;
         }
