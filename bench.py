@@ -293,7 +293,7 @@ def cpu_precision(patches, proposals, results, n_check=4):
                 w["chi2_relerr_max"] = max(w["chi2_relerr_max"], diff / max(abs(vals[ref][0][b]), 1e-3 * sc))
                 w["chi2_err_over_scale_max"] = max(w["chi2_err_over_scale_max"], diff / sc)
             gap = abs(c_g[b] - cref[b])
-            gap_explained &= bool(gap <= abs(cref[b] - c64[b]) + 1e-6 * abs(c64[b]))
+            gap_explained &= bool(gap <= abs(cref[b] - c64[b]) + 1e-6 * max(abs(c64[b]), 1e-3 * sc))
         for name, (a, ref) in pairs.items():
             ga, gr = vals[a][1], vals[ref][1]
             for k in range(7):

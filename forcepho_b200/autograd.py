@@ -134,7 +134,9 @@ class BatchChi2(torch.nn.Module):
         fl = r.reshape(-1).index_select(0, self._flux_src).to(torch.float64)
         out.index_copy_(0, self._flux_param, fl * g2.index_select(0, self._flux_src // (MAXSOURCES * NPARAMS)))
         # shape parameters: summed over the bands with their weights
-        w = torch.einsum("pb,pbsk->psk", g2.view(self.n, MAXBANDS), r[..., 1:].to(torch.float64))
+        # (elementwise products and a sum: no library GEMM, so no handle or
+        # workspace to create inside a graph capture)
+        w = (g2.view(self.n, MAXBANDS, 1, 1) * r[..., 1:].to(torch.float64)).sum(dim=1)
         out.index_copy_(0, self._shape_param, w.reshape(-1).index_select(0, self._shape_src))
         return out
 

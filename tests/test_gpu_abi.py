@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tolerances import CHI2_F64, GRAD_F64, band_scales, chi2_raw_err, grad_err
+from tolerances import (CHI2_F64, CHI2_REF, GRAD_F64, GRAD_REF, band_scales, chi2_err, chi2_raw_err, chi2_scale,
+                        grad_err)
 
 pytestmark = pytest.mark.gpu
 
@@ -160,5 +161,9 @@ def test_plain_comparator_still_matches():
     torch.cuda.synchronize()
     c_p = chi2.cpu().numpy()
     g_p = resp.cpu().numpy().reshape(nb, MAXSOURCES, NPARAMS)[:, :ns]
-    assert np.max(np.abs(c_p - chi2_t) / np.abs(chi2_t)) < 1e-5
-    assert grad_err(g_p, g_t) < 1e-4
+    # the comparator computes in FP32 like the reference kernel, whose raw chi2
+    # error can pass 1e-5 where chi2 has cancelled; its tolerance is the
+    # reference's, relative to sum (r^2 + d^2) ierr^2
+    _, _, r64 = O.evaluate(p, prop, precision="f64", return_residual=True)
+    assert chi2_err(c_p, chi2_t, chi2_scale(chi2_t, p.data, p.ierr, r64)) < CHI2_REF
+    assert grad_err(g_p, g_t) < GRAD_REF

@@ -39,7 +39,7 @@ def test_max_bands_and_sources(kind):
     tol_c, tol_g = (CHI2_F64, GRAD_F64) if kind == "tiled" else (CHI2_REF, GRAD_REF)
     assert chi2_err(chi2, c64, sc) < tol_c
     assert chi2_raw_err(chi2, c64, band_scales(p, r64)) < tol_c
-    assert ref_gap_explained(chi2, cr, c64, tol_c)
+    assert ref_gap_explained(chi2, cr, c64, tol_c, band_scales(p, r64))
     assert grad_err(dchi2, g64) < tol_g
     scale = float(np.max(np.abs(r64)))
     assert np.max(np.abs(res.astype(np.float64) - r64)) <= 1e-5 * scale

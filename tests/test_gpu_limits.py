@@ -59,7 +59,7 @@ def test_limits_parity(limits_patch, kind):
         grefe = grad_err(dchi2[b], gref[b])
         assert eref < CHI2_REF and grefe < GRAD_REF, (kind, b, eref, grefe)
         assert raw64 < tol_c and g64e < tol_g, (kind, b, raw64, g64e)
-        assert ref_gap_explained(chi2[b], cref[b], c64[b], tol_c), (kind, b, chi2[b], cref[b], c64[b])
+        assert ref_gap_explained(chi2[b], cref[b], c64[b], tol_c, sc), (kind, b, chi2[b], cref[b], c64[b])
 
 
 def test_limits_autograd_and_fd(limits_patch):

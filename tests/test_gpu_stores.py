@@ -32,7 +32,7 @@ def test_reference_image_patch_on_the_gpu():
         sc = band_scales(p, g["f64_residual_%d" % k])
         assert chi2_raw_err(chi2, g["f64_chi2_%d" % k], sc) < CHI2_F64
         assert grad_err(dchi2, g["f64_dchi2_%d" % k]) < GRAD_F64
-        assert ref_gap_explained(chi2, g["ref_chi2_%d" % k], g["f64_chi2_%d" % k])
+        assert ref_gap_explained(chi2, g["ref_chi2_%d" % k], g["f64_chi2_%d" % k], CHI2_F64, sc)
         assert grad_err(dchi2, g["ref_dchi2_%d" % k]) < 1e-4
         peak = np.abs(p.data.astype(np.float64) - g["f64_residual_%d" % k]).max()
         assert np.max(np.abs(res - g["f64_residual_%d" % k])) <= 1e-5 * peak

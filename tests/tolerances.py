@@ -77,14 +77,17 @@ def chi2_raw_err(chi2, chi2_ref, scales):
     return float(np.max(e)) if e.size else 0.0
 
 
-def ref_gap_explained(chi2, chi2_ref, chi2_f64, tol=CHI2_F64):
-    """Whether |chi2 - ref| <= |ref - f64| + tol |f64| in every band: the GPU
-    result's distance from the FP32 reference kernel is the reference's own
-    rounding error, up to the GPU's own tolerance."""
+def ref_gap_explained(chi2, chi2_ref, chi2_f64, tol=CHI2_F64, scales=0.0):
+    """Whether |chi2 - ref| <= |ref - f64| + tol max(|f64|, RAW_FLOOR scale)
+    in every band: the GPU result's distance from the FP32 reference kernel
+    is the reference's own rounding error, up to the GPU's own tolerance in
+    the raw metric (``scales``: per-band sum (r^2 + d^2) ierr^2, for bands
+    whose chi2 has cancelled)."""
     c = np.asarray(chi2, np.float64)
     r = np.asarray(chi2_ref, np.float64)
     f = np.asarray(chi2_f64, np.float64)
-    return bool(np.all(np.abs(c - r) <= np.abs(r - f) + tol * np.abs(f) + 1e-300))
+    den = np.maximum(np.abs(f), RAW_FLOOR * np.asarray(scales, np.float64))
+    return bool(np.all(np.abs(c - r) <= np.abs(r - f) + tol * den + 1e-300))
 
 
 def grad_err(g, gref):
