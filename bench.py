@@ -82,6 +82,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--tile-pixels", type=int, default=0)
+    ap.add_argument("--tile-classes", action="store_true", help="autotune a tile size per exposure-size class")
     return ap.parse_args()
 
 
@@ -469,7 +470,9 @@ def run_ours(args):
         p.send_to_device()
     proposals = perturbed_proposals(patches)
     tp = args.tile_pixels or 1024
-    tune = "classes" if not args.no_autotune and not args.tile_pixels else False
+    # one tile size for the batch (3 sizes x 2 CTA counts); the per-class tuner
+    # (--tile-classes) measured no gain on this workload
+    tune = False if args.no_autotune or args.tile_pixels else ("classes" if args.tile_classes else True)
     bp = BatchedProposer(patches, tile_pixels=tp, autotune=tune)
     bp.set_proposals_async(proposals)
     torch.cuda.synchronize()
@@ -531,7 +534,8 @@ def run_ours(args):
     achieved = FLOPS_PER_PAIR * active / (tile_ms * 1e-3) / 1e12
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_tflops.value, "unit": "TFLOP/s",
                 "frac": achieved / fp32_tflops.value,
-                "traffic": TILE_TRAFFIC.get((args.workload, args.patches, bp.tile_pixels)),
+                "traffic": (TILE_TRAFFIC.get((args.workload, args.patches, bp.tile_pixels))
+                            if len(bp.tile_classes) == 1 else None),
                 "kernel": "tile_kernel<%d>" % (bp.tile_pixels // 256),
                 "kernel_ms": tile_ms, "share_of_step": tile_ms / ms,
                 "peak_source": "measured in this run: FFMA-chain kernel (fp_measure_peaks), not in MEASURED_PEAKS.json",
