@@ -45,13 +45,16 @@ class _Chi2Fn(torch.autograd.Function):
     def forward(ctx, theta, owner):
         chi2, resp = owner._evaluate(theta.detach())
         ctx.owner = owner
+        ctx.theta_meta = (theta.device, theta.dtype)
         ctx.save_for_backward(resp)
         return chi2
 
     @staticmethod
     def backward(ctx, grad_chi2):
         (resp,) = ctx.saved_tensors
-        return ctx.owner._vjp(grad_chi2, resp), None
+        dev, dt = ctx.theta_meta
+        g = ctx.owner._vjp(grad_chi2.to(ctx.owner.device), resp)
+        return g.to(device=dev, dtype=dt), None
 
 
 class BatchChi2(torch.nn.Module):
