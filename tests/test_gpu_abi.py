@@ -167,3 +167,25 @@ def test_plain_comparator_still_matches():
     _, _, r64 = O.evaluate(p, prop, precision="f64", return_residual=True)
     assert chi2_err(c_p, chi2_t, chi2_scale(chi2_t, p.data, p.ierr, r64)) < CHI2_REF
     assert grad_err(g_p, g_t) < GRAD_REF
+
+
+def test_kernel_abi_plan_cache_evicts_and_replans():
+    """More patches than the library keeps plans for (64): the least recently
+    used plan is freed, and a later call on its patch re-plans and gives the
+    same bits."""
+    from forcepho_b200 import _native as N
+    from forcepho_b200 import synthetic as S
+    L = N.load()
+    assert L.fp_evaluate_proposal_release() == 0
+    patches = []
+    for i in range(66):
+        p = S.config_small(seed=100 + i, size=32)
+        p.return_residual = False
+        p.send_to_device()
+        patches.append(p)
+    props = [_perturbed(p) for p in patches]
+    first = [_call(L, p, q) for p, q in zip(patches, props)]      # 66 plans: the first two evicted
+    again = _call(L, patches[0], props[0])
+    assert np.array_equal(again[0], first[0][0]) and np.array_equal(again[1], first[0][1])
+    _check_f64(patches[0], props[0], *again)
+    assert L.fp_evaluate_proposal_release() == 0
