@@ -74,7 +74,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched",
-                    choices=["batched", "limits", "multiband", "small", "hmc", "nuts", "single", "precision"])
+                    choices=["batched", "limits", "multiband", "small", "hmc", "nuts", "single", "precision",
+                             "autograd"])
     ap.add_argument("--nuts-depth", type=int, default=6, help="max tree depth (nuts workload)")
     ap.add_argument("--hmc-steps", type=int, default=16, help="leapfrog steps per trajectory (hmc workload)")
     ap.add_argument("--patches", type=int, default=512)
@@ -844,6 +845,54 @@ def run_nuts_bench(args):
     print(json.dumps(out), flush=True)
 
 
+def run_autograd(args):
+    """The differentiable path: forward (chi2 per band) and backward (the
+    vector-Jacobian product) through ``PatchChi2`` on the limits patch (30
+    sources, 8 bands x 4 exposures of 256x256 px: 420 parameters) and through
+    ``BatchChi2`` on the batched workload's patches, timed with CUDA events
+    over --steps forward+backward passes after --warmup; theta stays on the
+    device throughout."""
+    import torch
+    from forcepho_b200 import synthetic as S
+    from forcepho_b200.autograd import BatchChi2, PatchChi2
+    torch.cuda.set_device(0)
+    out = {"metric": "forward+backward passes of the differentiable chi2", "unit": "pixel-Gaussian evals/s",
+           "steps": args.steps, "warmup": args.warmup, "data": "synthetic", "higher_is_better": True, "cases": {}}
+    lim = S.config_limits(seed=3)
+    lim.return_residual = False
+    lim.send_to_device()
+    import copy
+    bargs = copy.copy(args)
+    bargs.workload = "batched"
+    patches = make_patches(bargs, 0)
+    for p in patches:
+        p.return_residual = False
+        p.send_to_device()
+    for name, fn, pats in (("limits", PatchChi2(lim), [lim]), ("batched", BatchChi2(patches), patches)):
+        th = np.concatenate([p.scene.get_all_source_params() for p in pats])
+        theta = torch.tensor(th, dtype=torch.float64, device="cuda", requires_grad=True)
+        w = torch.ones(fn.n_rows, dtype=torch.float64, device="cuda")
+
+        def step():
+            theta.grad = None
+            (fn(theta) * w).sum().backward()
+
+        for _ in range(max(args.warmup, 3)):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        pairs = sum(p.n_pairs() for p in pats)
+        out["cases"][name] = {"patches": len(pats), "parameters": fn.n_params, "ms_per_pass": ms,
+                              "value": pairs / (ms * 1e-3), "pairs_per_pass": pairs}
+    print(json.dumps(out), flush=True)
+
+
 def run_single(args):
     """Single-patch call latency, as forcepho's own samplers call the kernel
     (one proposal per call, host proposal in, results out): the Python
@@ -992,6 +1041,8 @@ def main():
         run_single(args)
     elif args.workload == "precision":
         run_precision(args)
+    elif args.workload == "autograd":
+        run_autograd(args)
     else:
         run_ours(args)
 
