@@ -76,7 +76,12 @@ int check_rule(const fp_tile_rule *r)
     if (!r || r->n_classes < 1 || r->n_classes > FP_MAX_TILE_CLASSES)
         return fp_set_error(FP_ERR_ARGUMENT, "tile rule: n_classes must be in [1, %d]", FP_MAX_TILE_CLASSES);
     for (int c = 0; c < r->n_classes; ++c) {
-        if (int rc = check_tile_pixels(r->tile_pixels[c])) return rc;
+        const int tp = r->tile_pixels[c];
+        // a launch covers every class of its plan, so each must be a size the tile kernel runs
+        if (r->n_classes > 1 && tp != 256 && tp != 512 && tp != 1024)
+            return fp_set_error(FP_ERR_ARGUMENT, "tile rule: class %d has tile_pixels=%d (supported: 256, 512, 1024)",
+                                c, tp);
+        if (int rc = check_tile_pixels(tp)) return rc;
         if (c > 0 && c < r->n_classes - 1 && r->max_exposure_pixels[c] < r->max_exposure_pixels[c - 1])
             return fp_set_error(FP_ERR_ARGUMENT, "tile rule: class bounds must ascend");
     }

@@ -243,8 +243,11 @@ class StorePatchBase(B200PatchMixin, PatchBase):
         median source position unless given), in place, so that FP32
         proposals keep their precision (patch.py:427-461)."""
         if sky_zero is None:
-            sky_zero = np.array([np.median([s.ra for s in scene.sources]),
-                                 np.median([s.dec for s in scene.sources])])
+            if len(scene.sources) == 0:
+                sky_zero = self.patch_reference_coordinates
+            else:
+                sky_zero = np.array([np.median([s.ra for s in scene.sources]),
+                                     np.median([s.dec for s in scene.sources])])
         zero = np.array(sky_zero, dtype=np.float64)
         self.patch_reference_coordinates = zero
         for s in scene.sources:

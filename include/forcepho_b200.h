@@ -287,8 +287,9 @@ FP_API int fp_plan_count(const fp_patch_shape *h_shapes, int n_patches, int tile
  * all evaluated in the same persistent launch.  An exposure of n pixels takes
  * the first class c with n <= max_exposure_pixels[c] (the last class takes
  * every larger one) and is split into tiles of tile_pixels[c] pixels (cells of
- * the image plane as for fp_plan_count).  The kernels support 256, 512 and
- * 1024; the launch's tile_pixels must be the largest class of the plan. */
+ * the image plane as for fp_plan_count).  With more than one class each
+ * class's size must be one the kernels run (256, 512 or 1024; FP_ERR_ARGUMENT
+ * otherwise); the launch's tile_pixels must be the largest class of the plan. */
 #define FP_MAX_TILE_CLASSES 4
 typedef struct fp_tile_rule {
     int32_t n_classes;                               /* 1 .. FP_MAX_TILE_CLASSES */

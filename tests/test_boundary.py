@@ -219,6 +219,9 @@ def test_planner_tile_rule_classes():
     N.check(L.fp_plan_count_rule(ctypes.addressof(arr), len(shapes), ctypes.byref(N.tile_rule([(0, 512)])),
                                  ctypes.byref(sz2)), "count")
     assert sz1.n_tiles == sz2.n_tiles and sz1.n_partials == sz2.n_partials
+    odd = N.tile_rule([(4096, 256), (16384, 768)])       # a multiple of 32 the kernel does not run
+    assert L.fp_plan_count_rule(ctypes.addressof(arr), len(shapes), ctypes.byref(odd), ctypes.byref(sz)) \
+        == N.FP_ERR_ARGUMENT
     bad = N.tile_rule([(4096, 256), (16384, 500)])
     assert L.fp_plan_count_rule(ctypes.addressof(arr), len(shapes), ctypes.byref(bad), ctypes.byref(sz)) \
         == N.FP_ERR_ARGUMENT
