@@ -16,6 +16,10 @@ Modules, with the reference counterparts they stand in for:
 * ``stores``      -- ``FITSPatch``, ``StorePatch``, ``PSFStore``, regions, and the FITS, TAN-WCS
                      and HDF5 readers (``forcepho.patches.pixel_patch``, ``storage``, ``forcepho.region``)
 * ``distributed`` -- ``PatchFarm``: patches shared out over processes / GPUs
+* ``superscene``  -- ``SuperScene`` / ``LinkedSuperScene``: the field's catalog, regions checked
+                     out of and into it, prior bounds (``forcepho.superscene``)
+* ``dispatcher``  -- rounds of checked-out regions worked as batches on every GPU
+                     (``forcepho.dispatcher``)
 * ``sources``, ``patch``, ``structs``, ``kernel_limits``, ``splines`` -- the data
   model (``forcepho.sources``, ``forcepho.patches.patch``, ``forcepho.kernel_limits``)
 * ``synthetic``   -- seeded synthetic patches of the benchmark workloads

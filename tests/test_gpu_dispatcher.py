@@ -1,0 +1,89 @@
+"""The dispatcher's GPU work unit end to end: a field of sources in a FITS
+image set, a SuperScene over their catalog, rounds of regions packed from the
+images, fixed sources subtracted on the device, fluxes solved, and chi2 and
+gradients of each round's patches from one batched launch, checked against
+the FP64 oracle on the same packed patches."""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tolerances import CHI2_F64, GRAD_F64, band_scales, chi2_raw_err, grad_err
+
+pytestmark = pytest.mark.gpu
+
+BANDS = ["B0", "B1"]
+
+
+def _field(rng, n=12):
+    from forcepho_b200 import superscene as SS
+    cat = np.zeros(n, dtype=SS.sourcecat_dtype(bands=BANDS))
+    # within the 120 x 96 pixel (3.6" x 2.9") images around (53.1, -27.8)
+    dx, dy = rng.uniform(-1.4, 1.4, n), rng.uniform(-1.1, 1.1, n)
+    cat["ra"] = 53.1 + dx / 3600. / np.cos(np.deg2rad(-27.8))
+    cat["dec"] = -27.8 + dy / 3600.
+    cat["q"], cat["pa"] = rng.uniform(0.5, 0.9, n), rng.uniform(-1, 1, n)
+    cat["sersic"], cat["rhalf"] = rng.uniform(1.2, 3.5, n), rng.uniform(0.05, 0.12, n)
+    cat["roi"] = 3 * cat["rhalf"]
+    for b in BANDS:
+        cat[b] = rng.uniform(100, 300, n)
+    return cat
+
+
+def test_flux_fit_rounds_on_a_fits_field(tmp_path):
+    from test_stores import _PSF, make_image_set
+    from forcepho_b200 import dispatcher as D
+    from forcepho_b200 import superscene as SS
+    from forcepho_b200.stores.patch import FITSPatch
+
+    rng = np.random.default_rng(41)
+    paths = make_image_set(tmp_path, seed=9, size=(120, 96))
+    truth = _field(rng)
+
+    class TruthPatch(FITSPatch):
+        """Image noise plus the FP64 model of every true source."""
+
+        def build_patch(self, region=None, sourcecat=None, allbands=BANDS, tweak_background=False):
+            super().build_patch(region, None, allbands=allbands)
+            scene = self.set_scene(truth)
+            self.pack_meta(scene)
+            self.data = (self.data + O.render(self, scene.get_proposal())).astype(np.float32)
+            if sourcecat is not None:
+                self.pack_meta(self.set_scene(sourcecat))
+
+    def make_patcher():
+        p = TruthPatch(fitsfiles=paths)
+        p.psfstore = _PSF()
+        return p
+
+    cat = truth.copy()
+    for b in BANDS:
+        cat[b] *= rng.uniform(0.7, 1.3, len(cat))       # starting fluxes off the truth
+    start = cat.copy()                                  # the scene updates cat in place
+    scene = SS.SuperScene(sourcecat=cat, bands=BANDS, maxactive_per_patch=4, maxradius=0.6, boundary_radius=0.8,
+                          nscale=3, minradius=0.15, target_niter=1, maxactive_fraction=0.9,
+                          rng=np.random.default_rng(5))
+    work = D.flux_fit_work(make_patcher, BANDS, keep_patches=True)
+    checked = []
+
+    def checked_work(tasks):
+        res = work(tasks)
+        for t, r in zip(tasks, res):
+            p = r.pop("patch")
+            prop = p.scene.get_proposal()
+            c64, g64, r64 = O.evaluate(p, prop, precision="f64", return_residual=True)
+            assert chi2_raw_err(r["chi2"], c64, band_scales(p, r64)) < CHI2_F64
+            assert grad_err(r["dchi2"], g64) < GRAD_F64
+            checked.append(t["taskid"])
+            p.free()
+        return res
+
+    rounds = D.run(scene, checked_work, batch_per_rank=4, max_rounds=20)
+    assert len(checked) == sum(r["tasks"] for r in rounds) > 0
+    done = scene.sourcecat["n_iter"] >= 1
+    assert done.sum() >= len(cat) // 2
+    # fitted fluxes sit closer to the truth than the starting ones
+    for b in BANDS:
+        err0 = np.abs(start[b][done] - truth[b][done])
+        err1 = np.abs(scene.sourcecat[b][done] - truth[b][done])
+        assert np.median(err1) < np.median(err0)
