@@ -28,6 +28,8 @@ A patch provides ``set_scene(catalog)`` and ``meta_for(scene)`` /
 ``synthetic.SyntheticPatch`` does for the synthetic workloads).
 """
 
+import copy
+
 import numpy as np
 import torch
 
@@ -108,6 +110,25 @@ def _forward_only(views, proposals, ctas_per_sm=4):
     return plan
 
 
+def _scene_view(patch, scene, data_ptr, residual_ptr):
+    """A SceneView of ``scene`` (from ``patch.set_scene``) and the scene, with
+    its positions as the offsets the metadata and proposals take.  A
+    store-backed patch's ``set_scene`` gives absolute positions (its
+    ``pack_meta`` zeroes them): the scene is zeroed at its own median, as the
+    reference's ``pack_meta`` does for every scene it renders, and the patch's
+    own reference coordinate is left as it was.  A synthetic patch's catalog
+    already holds offsets."""
+    if not hasattr(patch, "zerocoords"):
+        return SceneView(patch, scene, data_ptr, residual_ptr), scene
+    saved = np.array(patch.patch_reference_coordinates, dtype=np.float64, copy=True)
+    try:
+        patch.zerocoords(scene)
+        view = SceneView(patch, scene, data_ptr, residual_ptr)
+    finally:
+        patch.patch_reference_coordinates = saved
+    return view, scene
+
+
 def _scene_proposal(scene):
     srcs = list(scene.sources)
     if not srcs:
@@ -171,8 +192,11 @@ def design_models(patch, active):
         return X[:, :patch.npix], scene
     zeros = torch.zeros(max(patch.npix, 1), dtype=torch.float32, device=dev)
     from .sources import Scene
-    views = [SceneView(patch, Scene([g]), zeros.data_ptr(), X[i].data_ptr()) for i, g in enumerate(scene.sources)]
-    props = [_scene_proposal(Scene([g])) for g in scene.sources]
+    views, props = [], []
+    for i, g in enumerate(scene.sources):
+        v, one = _scene_view(patch, Scene([copy.copy(g)]), zeros.data_ptr(), X[i].data_ptr())
+        views.append(v)
+        props.append(_scene_proposal(one))
     plan = _forward_only(views, props)
     X.neg_()                                             # residual of zero data = -model
     flux = torch.tensor(np.array([g.flux for g in scene.sources], dtype=np.float64),
@@ -227,7 +251,7 @@ def render(patch, catalog, splinedata=None, unpack=True):
     npix = max(patch.npix, 1)
     zeros = torch.zeros(npix, dtype=torch.float32, device=dev)
     out = torch.empty(npix, dtype=torch.float32, device=dev)
-    view = SceneView(patch, scene, zeros.data_ptr(), out.data_ptr())
+    view, scene = _scene_view(patch, scene, zeros.data_ptr(), out.data_ptr())
     plan = _forward_only([view], [_scene_proposal(scene)])
     del plan, view
     model = (-out[:patch.npix]).cpu().numpy()

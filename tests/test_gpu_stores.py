@@ -91,3 +91,32 @@ def test_packed_fits_set_in_a_batch_with_synthetic_patches(tmp_path):
         c64, g64, r64 = O.evaluate(x, prop, precision="f64", return_residual=True)
         assert chi2_raw_err(chi2, c64, band_scales(x, r64)) < CHI2_F64
         assert grad_err(dchi2, g64) < GRAD_F64
+
+
+def test_render_and_flux_solve_on_a_packed_fits_patch(tmp_path):
+    """Store-backed patches take catalogs in absolute coordinates: the GPU
+    render and the design matrix of one must match the FP64 model of the
+    packed scene, and a noiseless flux solve must return the catalog fluxes."""
+    from test_stores import _PSF, make_image_set
+    from forcepho_b200.fitting import optimize_fluxes
+    from forcepho_b200.stores.patch import FITSPatch
+    from forcepho_b200.stores.region import CircularRegion
+    paths = make_image_set(tmp_path, seed=8)
+    p = FITSPatch(fitsfiles=paths)
+    p.psfstore = _PSF()
+    cat = np.zeros(2, dtype=[(c, np.float64) for c in ("ra", "dec", "q", "pa", "sersic", "rhalf", "B0", "B1")])
+    cat["ra"], cat["dec"] = [53.1, 53.1 + 4e-5], [-27.8, -27.8 + 2e-5]
+    cat["q"], cat["pa"], cat["sersic"], cat["rhalf"] = [0.8, 0.5], [0.2, 1.0], [2.5, 1.2], [0.12, 0.2]
+    cat["B0"], cat["B1"] = [20.0, 8.0], [15.0, 6.0]
+    p.build_patch(CircularRegion(53.1, -27.8, 0.6 / 3600.0), cat, allbands=["B0", "B1"])
+    want = O.render(p, p.scene.get_proposal())
+    p.return_residual = True
+    p.send_to_device()
+    got = np.concatenate(p.render(cat))
+    assert np.max(np.abs(got - want)) <= 1e-5 * np.max(np.abs(want))
+    live = p.ierr > 0
+    p.data = np.where(live, want, 0.0).astype(np.float32)
+    p.send_to_device()
+    fluxes, precisions = optimize_fluxes(p, cat)
+    for b, name in enumerate(p.bandlist):
+        np.testing.assert_allclose(fluxes[b], cat[name], rtol=1e-4)
