@@ -80,10 +80,11 @@ def test_flux_fit_rounds_on_a_fits_field(tmp_path):
             off = prop.copy()
             off["fluxes"] *= 1.05
             off["q"] = np.clip(off["q"] * 0.95, 0.2, 0.99)
-            # about a pixel: far enough that the FP32 rounding of the pixel
-            # coordinates (4e-6 px at x ~ 100) is small beside the offset
-            off["ra"] += 1e-5
-            off["dec"] -= 1e-5
+            # about 5 pixels: the FP32 pixel coordinates and Gaussian centres
+            # (rounding up to 4e-6 px at x ~ 100) move chi2 and its position
+            # gradient by that much; far from the mode it is small beside them
+            off["ra"] += 4e-5
+            off["dec"] -= 4e-5
             c, g = B200Proposer().evaluate_proposal(off, patch=p)[:2]
             c64, g64, r64 = O.evaluate(p, off, precision="f64", return_residual=True)
             assert chi2_raw_err(c, c64, band_scales(p, r64)) < CHI2_F64
