@@ -40,6 +40,9 @@ METRIC = ("lnlike+grad evals/s and pixel-Gaussian evals/s (batched vs plain, 1 B
 UNIT = "pixel-Gaussian evals/s"
 FLOPS_PER_PAIR = 84      # FP32 flops (FMA = 2) of one forward + adjoint pair evaluation
 EX2_PER_PAIR = 2
+# raw chi2 errors of a band are measured against max(|chi2|, RAW_FLOOR * the
+# band's sum (r^2 + d^2) ierr^2), as the parity tests measure them
+RAW_FLOOR = 1e-2
 
 
 # DRAM bytes (read + write) of one tile_kernel launch, measured by ncu
@@ -265,7 +268,7 @@ def cpu_precision(patches, proposals, results, n_check=4):
     from the timed batch (``precision_sample``), with the exact inputs the GPU
     saw, evaluated by the FP64 oracle and by the reference CPU kernel.
 
-    chi2 errors are raw, |dchi2| / |chi2| per band (with the floor 1e-3 of
+    chi2 errors are raw, |dchi2| / |chi2| per band (with the floor RAW_FLOOR of
     sum (r^2 + d^2) ierr^2 for bands whose chi2 has cancelled), and scaled,
     |dchi2| / sum (r^2 + d^2) ierr^2; gradient errors per parameter column,
     normwise.  Three comparisons on the same patches: GPU vs FP64, GPU vs the
@@ -293,10 +296,10 @@ def cpu_precision(patches, proposals, results, n_check=4):
             for name, (a, ref) in pairs.items():
                 diff = abs(vals[a][0][b] - vals[ref][0][b])
                 w = worst[name]
-                w["chi2_relerr_max"] = max(w["chi2_relerr_max"], diff / max(abs(vals[ref][0][b]), 1e-3 * sc))
+                w["chi2_relerr_max"] = max(w["chi2_relerr_max"], diff / max(abs(vals[ref][0][b]), RAW_FLOOR * sc))
                 w["chi2_err_over_scale_max"] = max(w["chi2_err_over_scale_max"], diff / sc)
             gap = abs(c_g[b] - cref[b])
-            gap_explained &= bool(gap <= abs(cref[b] - c64[b]) + 1e-6 * max(abs(c64[b]), 1e-3 * sc))
+            gap_explained &= bool(gap <= abs(cref[b] - c64[b]) + 1e-6 * max(abs(c64[b]), RAW_FLOOR * sc))
         for name, (a, ref) in pairs.items():
             ga, gr = vals[a][1], vals[ref][1]
             for k in range(7):
@@ -305,7 +308,7 @@ def cpu_precision(patches, proposals, results, n_check=4):
                     worst[name]["grad_colnorm_relerr_max"] = max(
                         worst[name]["grad_colnorm_relerr_max"], float(np.linalg.norm(ga[..., k] - gr[..., k]) / den))
     out = {"patches": picked, "pairs_per_patch": [int(patches[i].n_pairs()) for i in picked],
-           "chi2_relerr": "max over bands of |dchi2| / max(|chi2|, 1e-3 sum (r^2+d^2) ierr^2)",
+           "chi2_relerr": "max over bands of |dchi2| / max(|chi2|, 1e-2 sum (r^2+d^2) ierr^2)",
            "gpu_gap_to_reference_within_reference_error": gap_explained}
     out.update(worst)
     # the names of earlier records
@@ -605,7 +608,7 @@ def run_ours(args):
             s1 = int(p.exposure_start[e0 + ne - 1] + p.exposure_N[e0 + ne - 1])
             # chi2 = sum (r^2 - d^2) ierr^2, so sum (r^2 + d^2) ierr^2 = chi2 + 2 sum d^2 ierr^2
             sc_b = float(c_b[b]) + 2.0 * float(np.sum(dd[s0:s1]))
-            worst_raw = max(worst_raw, abs(float(c_b[b]) - float(c_p[b])) / max(abs(float(c_b[b])), 1e-3 * sc_b,
+            worst_raw = max(worst_raw, abs(float(c_b[b]) - float(c_p[b])) / max(abs(float(c_b[b])), RAW_FLOOR * sc_b,
                                                                                   1e-300))
         den = np.linalg.norm(g_b) + 1e-30
         worst_g = max(worst_g, float(np.linalg.norm(g_b - g_p) / den))

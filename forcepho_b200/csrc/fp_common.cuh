@@ -31,6 +31,7 @@ int fp_sm_count(int *out);
 // [0, 256)                        : control block (queue counter, status)
 // gauss_fwd  float4[2*n_gauss]    : (xc, yc, c fxx, c fxy), (c fyy, amp k0, amp C24, k0)
 // gauss_box  float4[n_gauss]      : xmin, xmax, ymin, ymax of the E <= 36 box
+// gauss_ctr  float2[n_gauss]      : xc - (float)xc, yc - (float)yc: what the FP32 centre lost
 // gauss_jac  double[FP_JAC*n_gauss]
 // partials   double[n_partials]
 #define FP_JAC 20                   // amp, fxx, fxy, fyy, 15 Jacobian terms, pad
@@ -41,7 +42,7 @@ struct fp_control {
 };
 
 struct fp_workspace_layout {
-    size_t gauss_fwd, gauss_box, gauss_jac, partials, total;
+    size_t gauss_fwd, gauss_box, gauss_ctr, gauss_jac, partials, total;
 };
 
 static inline size_t fp_align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -52,6 +53,7 @@ static inline fp_workspace_layout fp_layout(int64_t n_gauss, int64_t n_partials)
     size_t off = fp_align256(sizeof(fp_control));
     L.gauss_fwd = off; off = fp_align256(off + (size_t)n_gauss * 2 * 16);
     L.gauss_box = off; off = fp_align256(off + (size_t)n_gauss * 16);
+    L.gauss_ctr = off; off = fp_align256(off + (size_t)n_gauss * 8);
     L.gauss_jac = off; off = fp_align256(off + (size_t)n_gauss * FP_JAC * 8);
     L.partials = off;  off = fp_align256(off + (size_t)n_partials * 8);
     L.total = off;

@@ -78,7 +78,7 @@ constexpr int FP_MAX_REPLICAS = 8;
 __global__ void __launch_bounds__(256)
 setup_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc *__restrict__ expos,
              const fp_source *__restrict__ proposals, float4 *__restrict__ gfwd,
-             float4 *__restrict__ gbox, double *__restrict__ gjac, fp_control *ctl)
+             float4 *__restrict__ gbox, float2 *__restrict__ gctr, double *__restrict__ gjac, fp_control *ctl)
 {
     const fp_exposure_desc ed = expos[blockIdx.x];
     const fp_patch *pt = patches[ed.patch];
@@ -93,6 +93,7 @@ setup_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc
             gfwd[2 * i] = make_float4(0.f, 0.f, 0.f, 0.f);
             gfwd[2 * i + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
             gbox[i] = make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY);
+            gctr[i] = make_float2(0.f, 0.f);
             double *J = gjac + (size_t)FP_JAC * i;
             for (int k = 0; k < FP_JAC; ++k) J[k] = 0.0;
         }
@@ -109,6 +110,11 @@ setup_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc
         const double k0 = 1.0 - (G.fxx + G.fyy) / 24.0;
         gfwd[2 * i] = make_float4(xc, yc, fxs, fxys);
         gfwd[2 * i + 1] = make_float4(fys, (float)(G.amp * k0), (float)(G.amp * FP_C24), (float)k0);
+        // what rounding the centre to FP32 lost (up to 6e-8 of the pixel
+        // coordinates): the tiles add it back to the centre relative to their
+        // own origin
+        const float xlo = (float)(G.xcen - (double)xc), ylo = (float)(G.ycen - (double)yc);
+        gctr[i] = make_float2(xlo, ylo);
 
         // box of {E <= MAX_EXP_ARG} for the FP32 parameters the pixel loops use,
         // widened by 1% in E and 1e-3 px so FP32 rounding of E cannot reach past it
@@ -117,7 +123,8 @@ setup_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc
         float4 box = make_float4(-INFINITY, INFINITY, -INFINITY, INFINITY);   // never culled
         if (isfinite(xc) && isfinite(yc) && isfinite(det) && det > 0.0 && Fxx > 0.0 && Fyy > 0.0) {
             const double lim = MAX_EXP_ARG * 1.01;
-            const double hx = sqrt(lim * Fyy / det) + 1e-3, hy = sqrt(lim * Fxx / det) + 1e-3;
+            const double hx = sqrt(lim * Fyy / det) + 1e-3 + fabs((double)xlo);
+            const double hy = sqrt(lim * Fxx / det) + 1e-3 + fabs((double)ylo);
             box = make_float4(__double2float_rd((double)xc - hx), __double2float_ru((double)xc + hx),
                               __double2float_rd((double)yc - hy), __double2float_ru((double)yc + hy));
         }
@@ -199,15 +206,44 @@ __global__ void pack_kernel(const fp_patch *const *__restrict__ patches,
     }
 }
 
+// The first pixel-loop parameter float4 of Gaussian gi, (xc, yc, c Fxx, c Fxy),
+// with its centre taken relative to a tile origin (ox, oy): the FP32 centre
+// minus the origin (exact for a Gaussian near the tile), plus what rounding
+// the centre to FP32 lost.  Pixel coordinates are taken relative to the same
+// origin, so dx = x - xc carries the rounding of |xc - ox|, not of |xc|: the
+// pixel coordinates of a large image (thousands of pixels, ulp 1e-4 px) no
+// longer limit the model's precision.
+__device__ __forceinline__ float4 stage_gauss(const float4 *__restrict__ gfwd, const float2 *__restrict__ gctr,
+                                              int64_t gi, float ox, float oy)
+{
+    float4 A = gfwd[2 * gi];
+    const float2 lo = gctr[gi];
+    A.x = (A.x - ox) + lo.x;
+    A.y = (A.y - oy) + lo.y;
+    return A;
+}
+
+// The origin of a tile's relative coordinates: its box centre, rounded to an
+// integer so that integer pixel coordinates stay exact; 0 for a box that is
+// not finite.
+__device__ __forceinline__ float2 tile_origin(const fp_tile &tl)
+{
+    const float ox = rintf(0.5f * (tl.bbox[0] + tl.bbox[1])), oy = rintf(0.5f * (tl.bbox[2] + tl.bbox[3]));
+    return make_float2(isfinite(ox) ? ox : 0.f, isfinite(oy) ? oy : 0.f);
+}
+
 // Forward pass of one tile, P pixels per thread (the tile holds at most
 // 256 P pixels): the model of each pixel over the tile's kept Gaussians, the
 // residual (written out when the patch has a residual array), the chi2 terms
 // reduced into s_red[FP_WARPS], and the nonzero-weight pixels (x, y, w) compacted
 // into s_pix in ascending order.  Returns their count (the same on every thread).
+// Pixel coordinates and Gaussian centres are taken relative to the tile's
+// origin (ox, oy) (stage_gauss); the boxes stay absolute.
 template <int P>
 __device__ __forceinline__ int forward_tile(const fp_tile &tl, const fp_exposure_desc &ed, const fp_patch *pt,
                                             const int32_t *__restrict__ perm, const float4 *__restrict__ pix,
                                             const float4 *__restrict__ gfwd, const float4 *__restrict__ gbox,
+                                            const float2 *__restrict__ gctr, const float ox, const float oy,
                                             const bool nocull, const int gc, const uint16_t *s_idx, float4 *s_ga,
                                             float4 *s_gb, float4 *s_gbox, float4 *s_pix, int *s_int, double *s_red)
 {
@@ -260,6 +296,11 @@ __device__ __forceinline__ int forward_tile(const fp_tile &tl, const fp_exposure
         wy1 = fmaxf(wy1, __shfl_xor_sync(0xffffffffu, wy1, o));
     }
     if (nocull) { wx0 = wy0 = -INFINITY; wx1 = wy1 = INFINITY; }
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+        xs[k] -= ox;
+        ys[k] -= oy;
+    }
     // one row: every thread's pixels share their y (cell rows in row order),
     // so the y-dependent products of a Gaussian are formed once per thread
     bool same_y = true;
@@ -281,7 +322,7 @@ __device__ __forceinline__ int forward_tile(const fp_tile &tl, const fp_exposure
         __syncthreads();
         for (int i = tid; i < cn; i += FP_THREADS) {
             const int64_t gi = ed.gauss_offset + s_idx[c0 + i];
-            s_ga[i] = gfwd[2 * gi];
+            s_ga[i] = stage_gauss(gfwd, gctr, gi, ox, oy);
             s_gb[i] = gfwd[2 * gi + 1];
             s_gbox[i] = gbox[gi];
         }
@@ -600,7 +641,7 @@ __global__ void __launch_bounds__(FP_THREADS, 4)
 tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc *__restrict__ expos,
             const fp_tile *__restrict__ tiles, const int32_t *__restrict__ order,
             const int32_t *__restrict__ perm, const float4 *__restrict__ pix, int64_t n_tiles,
-            const float4 *__restrict__ gfwd, const float4 *__restrict__ gbox,
+            const float4 *__restrict__ gfwd, const float4 *__restrict__ gbox, const float2 *__restrict__ gctr,
             const double *__restrict__ gjac, double *__restrict__ partials, fp_control *ctl,
             int max_gauss, int flags)
 {
@@ -639,6 +680,8 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
         const fp_exposure_desc ed = expos[tl.expo];
         const fp_patch *pt = patches[ed.patch];
         const int ng = ed.n_gauss, ns = ed.n_sources, n_psf = ed.n_psf;
+        const float2 org = tile_origin(tl);
+        const float ox = org.x, oy = org.y;
         const int npix = tl.n_pix;
         double *out = partials + tl.partial_offset;
         const int tp = tl.tile_pixels;
@@ -700,14 +743,14 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
         // ---- 2. forward: the tile's pixel class sets the pixels per thread ----
         int nzt;
         if (tl.tile_pixels == 1024)
-            nzt = forward_tile<4>(tl, ed, pt, perm, pix, gfwd, gbox, nocull, gc, s_idx, s_ga, s_gb, s_gbox, s_pix,
-                                  s_int, s_red);
+            nzt = forward_tile<4>(tl, ed, pt, perm, pix, gfwd, gbox, gctr, ox, oy, nocull, gc, s_idx, s_ga,
+                                  s_gb, s_gbox, s_pix, s_int, s_red);
         else if (tl.tile_pixels == 512)
-            nzt = forward_tile<2>(tl, ed, pt, perm, pix, gfwd, gbox, nocull, gc, s_idx, s_ga, s_gb, s_gbox, s_pix,
-                                  s_int, s_red);
+            nzt = forward_tile<2>(tl, ed, pt, perm, pix, gfwd, gbox, gctr, ox, oy, nocull, gc, s_idx, s_ga,
+                                  s_gb, s_gbox, s_pix, s_int, s_red);
         else
-            nzt = forward_tile<1>(tl, ed, pt, perm, pix, gfwd, gbox, nocull, gc, s_idx, s_ga, s_gb, s_gbox, s_pix,
-                                  s_int, s_red);
+            nzt = forward_tile<1>(tl, ed, pt, perm, pix, gfwd, gbox, gctr, ox, oy, nocull, gc, s_idx, s_ga,
+                                  s_gb, s_gbox, s_pix, s_int, s_red);
         for (int t = tid; t < FP_WARPS * MAXSOURCES * NPARAMS; t += FP_THREADS) s_wsrc[t] = 0.0;
 
         FP_PHASE_MARK(ph2);
@@ -718,7 +761,7 @@ tile_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc 
             if (gc > FP_CHUNK) {
                 for (int i = tid; i < cn; i += FP_THREADS) {
                     const int64_t gi = ed.gauss_offset + s_idx[c0 + i];
-                    s_ga[i] = gfwd[2 * gi];
+                    s_ga[i] = stage_gauss(gfwd, gctr, gi, ox, oy);
                     s_gb[i] = gfwd[2 * gi + 1];
                 }
             }
@@ -860,15 +903,18 @@ reduce_kernel(const fp_band_desc *__restrict__ bands, const fp_tile *__restrict_
 // pair census (diagnostic): how many (pixel, Gaussian) pairs the culled tile
 // kernel evaluates, how many lie within the MAX_EXP_ARG cutoff (the pairs that
 // change the result), and how many within-cutoff pairs belong to a Gaussian
-// the cull dropped (must be zero).  Same FP32 exponent as the pixel loops.
+// the cull dropped (must be zero).  Same FP32 exponent as the pixel loops, in
+// the same tile-relative coordinates.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 count_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc *__restrict__ expos,
              const fp_tile *__restrict__ tiles, const int32_t *__restrict__ perm,
-             const float4 *__restrict__ gfwd, const float4 *__restrict__ gbox, unsigned long long *counts)
+             const float4 *__restrict__ gfwd, const float4 *__restrict__ gbox, const float2 *__restrict__ gctr,
+             unsigned long long *counts)
 {
     extern __shared__ unsigned char s_keep[];   // [n_gauss]: the tile kernel's cull decision
     const fp_tile tl = tiles[blockIdx.x];
+    const float2 org = tile_origin(tl);
     const fp_exposure_desc ed = expos[tl.expo];
     const fp_patch *pt = patches[ed.patch];
     const float bx0 = tl.bbox[0], bx1 = tl.bbox[1], by0 = tl.bbox[2], by1 = tl.bbox[3];
@@ -883,11 +929,11 @@ count_kernel(const fp_patch *const *__restrict__ patches, const fp_exposure_desc
     unsigned long long inbox = 0, active = 0, bad = 0;
     for (int j = threadIdx.x; j < tl.n_pix; j += blockDim.x) {
         const int32_t ix = perm[tl.perm_start + j];
-        const float x = pt->xpix[ix], y = pt->ypix[ix];
+        const float x = pt->xpix[ix] - org.x, y = pt->ypix[ix] - org.y;
         for (int g = 0; g < ed.n_gauss; ++g) {
             const int64_t gi = ed.gauss_offset + g;
             const bool keep = s_keep[g] != 0;
-            const float4 A = gfwd[2 * gi], B = gfwd[2 * gi + 1];
+            const float4 A = stage_gauss(gfwd, gctr, gi, org.x, org.y), B = gfwd[2 * gi + 1];
             const float dx = x - A.x, dy = y - A.y;
             const float vx = fmaf(A.z, dx, A.w * dy);
             const float vy = fmaf(B.x, dy, A.w * dx);
@@ -922,7 +968,7 @@ std::atomic<bool> g_attr_set[ATTR_MAX_DEVICES][3];
 
 template <int P>
 int launch_tiles(int grid, size_t smem, cudaStream_t st, const fp_patch *const *d_patches,
-                 const fp_plan_tables &tb, int64_t n_tiles, const float4 *gfwd, const float4 *gbox,
+                 const fp_plan_tables &tb, int64_t n_tiles, const float4 *gfwd, const float4 *gbox, const float2 *gctr,
                  const double *gjac, double *partials, fp_control *ctl, int max_gauss, int flags)
 {
     int dev = 0;
@@ -941,7 +987,7 @@ int launch_tiles(int grid, size_t smem, cudaStream_t st, const fp_patch *const *
     }
     tile_kernel<P><<<grid, FP_THREADS, smem, st>>>(d_patches, tb.expos, tb.tiles, tb.order, tb.perm,
                                                     reinterpret_cast<const float4 *>(tb.pix), n_tiles,
-                                                    gfwd, gbox, gjac, partials, ctl, max_gauss, flags);
+                                                    gfwd, gbox, gctr, gjac, partials, ctl, max_gauss, flags);
     return fp_check_cuda(cudaGetLastError(), "tile_kernel launch");
 }
 
@@ -1009,7 +1055,8 @@ extern "C" int fp_count_pairs(const fp_patch *const *d_patches, const fp_plan_si
             return rc;
     count_kernel<<<(unsigned)sizes->n_tiles, 256, keep_bytes, (cudaStream_t)stream>>>(
         d_patches, tables->expos, tables->tiles, tables->perm, reinterpret_cast<const float4 *>(ws + L.gauss_fwd),
-        reinterpret_cast<const float4 *>(ws + L.gauss_box), d_counts);
+        reinterpret_cast<const float4 *>(ws + L.gauss_box), reinterpret_cast<const float2 *>(ws + L.gauss_ctr),
+        d_counts);
     return fp_check_cuda(cudaGetLastError(), "count_kernel launch");
 }
 
@@ -1072,13 +1119,14 @@ int run_batch(const batch_launch &a, const fp_patch *const *d_patches, const fp_
     fp_control *ctl = reinterpret_cast<fp_control *>(ws);
     float4 *gfwd = reinterpret_cast<float4 *>(ws + L.gauss_fwd);
     float4 *gbox = reinterpret_cast<float4 *>(ws + L.gauss_box);
+    float2 *gctr = reinterpret_cast<float2 *>(ws + L.gauss_ctr);
     double *gjac = reinterpret_cast<double *>(ws + L.gauss_jac);
     double *partials = reinterpret_cast<double *>(ws + L.partials);
 
     const int phases = launch->phases ? launch->phases : (FP_PHASE_SETUP | FP_PHASE_TILES | FP_PHASE_REDUCE);
     if ((phases & FP_PHASE_SETUP) && sizes->n_exposures > 0) {
         setup_kernel<<<(unsigned)sizes->n_exposures, 256, 0, st>>>(d_patches, tb.expos, d_proposals, gfwd, gbox,
-                                                                   gjac, ctl);
+                                                                   gctr, gjac, ctl);
         if (int rc = fp_check_cuda(cudaGetLastError(), "setup_kernel launch")) return rc;
     }
     if ((phases & FP_PHASE_TILES) && sizes->n_tiles > 0) {
@@ -1091,14 +1139,14 @@ int run_batch(const batch_launch &a, const fp_patch *const *d_patches, const fp_
         int rc;
         const int mg = (int)sizes->max_gauss;
         if (T == 256)
-            rc = launch_tiles<1>(grid, a.smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gjac, partials, ctl,
-                                 mg, launch->flags);
+            rc = launch_tiles<1>(grid, a.smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gctr, gjac, partials,
+                                 ctl, mg, launch->flags);
         else if (T == 512)
-            rc = launch_tiles<2>(grid, a.smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gjac, partials, ctl,
-                                 mg, launch->flags);
+            rc = launch_tiles<2>(grid, a.smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gctr, gjac, partials,
+                                 ctl, mg, launch->flags);
         else
-            rc = launch_tiles<4>(grid, a.smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gjac, partials, ctl,
-                                 mg, launch->flags);
+            rc = launch_tiles<4>(grid, a.smem, st, d_patches, tb, sizes->n_tiles, gfwd, gbox, gctr, gjac, partials,
+                                 ctl, mg, launch->flags);
         if (rc) return rc;
     }
     if ((phases & FP_PHASE_REDUCE) && sizes->n_band_outputs > 0) {

@@ -218,8 +218,11 @@ def test_mixed_tile_classes_in_one_launch(batch):
     assert len(tuned.tile_classes) == 3
     assert all(tp in (256, 512, 1024) for _, tp in tuned.tile_classes)
     res2 = tuned.evaluate_proposals(props)
-    for (c1, _), (c2, _), p in zip(res, res2, batch):
-        assert np.max(np.abs(c1 - c2) / np.maximum(np.abs(c1), 1e-300)) < 2 * CHI2_F64 or p.n_pairs() == 0
+    # tile sizes change the tile origins, hence each pair's FP32 rounding: the
+    # two plans agree to twice the tolerance each has against FP64
+    for (c1, _), (c2, _), p, prop in zip(res, res2, batch, props):
+        r64 = O.evaluate(p, prop, precision="f64", return_residual=True)[2]
+        assert chi2_raw_err(c2, c1, band_scales(p, r64)) < 2 * CHI2_F64
 
 
 def test_swapped_data_is_repacked_before_the_next_replay():
