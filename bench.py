@@ -1020,7 +1020,7 @@ def run_precision(args):
             d = p.data[s0:s1].astype(np.float64) * p.ierr[s0:s1]
             r = r64[s0:s1] * p.ierr[s0:s1]
             sc.append(float(np.sum(d * d + r * r)))
-        ce = [abs(chi2[b] - c64[b]) / max(abs(c64[b]), 1e-3 * s_) for b, s_ in zip(bl, sc)]
+        ce = [abs(chi2[b] - c64[b]) / max(abs(c64[b]), RAW_FLOOR * s_) for b, s_ in zip(bl, sc)]
         cols = component_errors(dchi2[bl], g64[bl])
         rows.append({"patch": name, "pairs": int(p.n_pairs()), "bands": bl, "chi2_relerr": ce,
                      "grad": dict(zip(["flux", "ra", "dec", "q", "pa", "sersic", "rhalf"], cols))})
