@@ -48,10 +48,10 @@ RAW_FLOOR = 1e-2
 # DRAM bytes (read + write) of one tile_kernel launch, measured by ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum, one pass, the first timed
 # launch of "bench.py --steps 2 --warmup 3 --no-cpu --no-autotune --tile-pixels
-# 1024 --plain-steps 1", NVTX range bench_timed): 4.238 GB read + 0.212 GB
+# 1024 --plain-steps 1", NVTX range bench_timed): 4.306 GB read + 0.212 GB
 # written.  Keyed by (workload, patches, tile pixels) of a one-size plan;
 # other configurations report null.
-TILE_TRAFFIC = {("batched", 512, 1024): 4.238219520e9 + 211.634688e6}
+TILE_TRAFFIC = {("batched", 512, 1024): 4.305974272e9 + 212.12416e6}
 
 
 def hbm_fraction(traffic_bytes, algorithmic_gbs, kernel_ms):
