@@ -25,7 +25,6 @@ scene evolves identically for any number of ranks with the same total batch.
 
 import time
 
-
 from .distributed import balance
 
 __all__ = ["checkout_batch", "task_weight", "run", "dummy_work", "flux_fit_work"]
