@@ -4,9 +4,15 @@
 // Per evaluation (all on one stream, no host synchronisation):
 //   setup_kernel   one CTA per exposure: every image Gaussian of the exposure in
 //                  FP64 (fp_gauss.cuh), stored as FP32 pixel-loop parameters with
-//                  the ex2 scale folded in, an FP32 bounding box of its
-//                  E = dx^T F dx <= MAX_EXP_ARG region, and the FP64 Jacobian.
-//   tile_kernel    persistent CTAs pop tiles (largest first).  Per tile:
+//                  the ex2 scale folded in, the FP32 centre's rounding residual,
+//                  an FP32 bounding box of its E = dx^T F dx <= MAX_EXP_ARG
+//                  region, and the FP64 Jacobian.
+//   tile_kernel    persistent CTAs pop tiles (largest first).  A tile takes
+//                  its pixel coordinates relative to the integer centre of its
+//                  box and rebuilds each Gaussian's centre there from the FP32
+//                  centre and its rounding residual, so FP32 offsets x - xc
+//                  do not lose the precision of large pixel coordinates.
+//                  Per tile:
 //                  1. cull: keep the Gaussians whose box, and then whose
 //                     E <= MAX_EXP_ARG ellipse (FP64), meets the tile's pixel
 //                     box; every other Gaussian has E > MAX_EXP_ARG at every
