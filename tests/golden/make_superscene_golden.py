@@ -179,7 +179,8 @@ def bounds(SS, cat, bands):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FORCEPHO_REF_ROOT", "/root/reference")
+    from oracle import oracle as O
+    root = sys.argv[1] if len(sys.argv) > 1 else O.reference_root()
     SS = import_reference(root)
     cat, bands = catalog(SS)
     gold = {"bands": bands, "catalog": {c: cat[c].tolist() for c in cat.dtype.names},
