@@ -24,7 +24,7 @@ import numpy as np
 import torch
 
 from . import _native as N
-from .device import Plan, current_stream_ptr, pack_proposals, response_view
+from .device import Plan, current_stream_ptr, response_view
 from .kernel_limits import MAXBANDS, MAXRADII, MAXSOURCES, NPARAMS
 from .structs import response_struct_dtype, source_struct_dtype
 
@@ -119,8 +119,7 @@ class B200Proposer(ProposerBase):
         if verbose:
             print("Launching tiled evaluation: %d tiles of %d px, %d CTAs/SM"
                   % (plan.sizes.n_tiles, plan.tile_pixels, self.ctas_per_sm), file=sys.stderr, flush=True)
-        host = pack_proposals([prop], 1)
-        self._pinned_prop.numpy()[:] = host.view(np.uint8).reshape(-1)
+        self._pinned_prop.numpy()[:prop.nbytes] = prop.view(np.uint8)     # n_sources records
         stream = torch.cuda.current_stream()
         lp = plan.launch(ctas_per_sm=self.ctas_per_sm, flags=self.flags)
         if self.use_graph:
@@ -143,11 +142,17 @@ class B200Proposer(ProposerBase):
         return chi_out, chi_derivs
 
     def _queue(self, plan, lp):
-        """Proposal upload, evaluation and read-back on the current stream."""
-        plan.proposals.copy_(self._pinned_prop, non_blocking=True)
+        """Proposal upload, evaluation and read-back on the current stream:
+        only the plan's source records and the patch's band rows cross PCIe
+        (the kernels read n_sources records and write n_bands rows)."""
+        patch = plan.patches[0]
+        nrec = int(patch.n_sources) * source_struct_dtype.itemsize
+        nb = patch.n_bands
+        if nrec:
+            plan.proposals[:nrec].copy_(self._pinned_prop[:nrec], non_blocking=True)
         plan.evaluate(lp)
-        self._pinned_chi2.copy_(plan.chi2, non_blocking=True)
-        self._pinned_resp.copy_(plan.response, non_blocking=True)
+        self._pinned_chi2[0, :nb].copy_(plan.chi2[0, :nb], non_blocking=True)
+        self._pinned_resp[0, :nb].copy_(plan.response[0, :nb], non_blocking=True)
 
     def _capture(self, plan, lp, stream):
         # one eager pass first sets the kernels' attributes outside the capture
