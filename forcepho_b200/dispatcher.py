@@ -20,14 +20,16 @@ scene evolves identically for any number of ranks with the same total batch.
 * ``dummy_work``      -- the reference's test work unit, without the sleep;
 * ``flux_fit_work``   -- a GPU work unit: pack each region's patch from the
   stores, subtract its fixed sources, solve the active sources' fluxes, and
-  evaluate chi2 and gradients of all the share's patches in one launch.
+  evaluate chi2 and gradients of all the share's patches in one launch;
+* ``hmc_work``        -- a GPU work unit that samples all the share's patches
+  together with device-resident HMC, as the reference's child samples one.
 """
 
 import time
 
 from .distributed import balance
 
-__all__ = ["checkout_batch", "task_weight", "run", "dummy_work", "flux_fit_work"]
+__all__ = ["checkout_batch", "task_weight", "run", "dummy_work", "flux_fit_work", "hmc_work"]
 
 
 def checkout_batch(scene, n_max, ntry=1000, first_taskid=0):
@@ -152,6 +154,98 @@ def flux_fit_work(make_patcher, allbands, niter=1, tile_pixels=256, keep_patches
                 r["patch"] = p
             else:
                 p.free()
+        return out
+
+    return work
+
+
+def _prepared_patch(make_patcher, task, allbands):
+    """The task region's patch on the device, fixed sources subtracted, the
+    active scene's metadata packed, no residual buffer; and that scene."""
+    p = make_patcher()
+    p.build_patch(task["region"], None, allbands=allbands)
+    if task["fixed"] is not None and len(task["fixed"]):
+        _, scene = p.subtract_fixed(task["fixed"], active=task["active"], swap_local=True)
+        p.device_ptrs.pop("residual", None)
+        p.return_residual = False
+        p.send_patchstruct_to_device()
+    else:
+        scene = p.set_scene(task["active"])
+        p.pack_meta(scene)
+        p.return_residual = False
+        p.send_to_device()
+    return p, scene
+
+
+def hmc_work(make_patcher, allbands, n_warmup=40, n_draws=40, n_steps=16, seed=0, tile_pixels=1024):
+    """A GPU sampling work unit over a share of regions: the counterpart of the
+    reference child's ``run_lmc`` on one patch (fitting.py:254-341), for all
+    the share's patches at once with ``hmc.DeviceHMC``.  Each region's patch is
+    packed, its fixed sources subtracted on the device, and its active
+    sources sampled within the task's prior bounds: step sizes adapted by
+    dual averaging over the first half of the ``n_warmup`` trajectories, the
+    diagonal mass matrix then taken from the second half's draws, then
+    ``n_draws`` recorded trajectories.  Each result carries ``final`` (the
+    active rows at the posterior mean), ``covs`` (per-source covariance of
+    the draws when the patch has every scene band), ``niter`` = n_draws, and
+    the acceptance rate of every patch."""
+    import numpy as np
+    import torch
+    from .hmc import DeviceHMC
+    from .superscene import bounds_vectors
+
+    def work(tasks):
+        patches, scenes, theta0, bounds = [], [], [], []
+        for t in tasks:
+            p, scene = _prepared_patch(make_patcher, t, allbands)
+            lo, hi = bounds_vectors(t["bounds"], p.bandlist, shapenames=t["shape_cols"],
+                                    reference_coordinates=p.patch_reference_coordinates)
+            patches.append(p)
+            scenes.append(scene)
+            theta0.append(np.clip(scene.get_all_source_params(), lo, hi))
+            bounds.append((lo, hi))
+        n1 = n_warmup // 2
+        n2 = n_warmup - n1
+        h = DeviceHMC(patches, theta0, bounds=bounds, n_steps=n_steps, max_traj=n_warmup + 2 * n_draws + 2,
+                      seed=seed, tile_pixels=tile_pixels)
+        h.estimate_inv_mass()
+        h.run(n1, adapt=True)
+        h.end_adaptation()
+        f64 = dict(dtype=torch.float64, device=h.device)
+        warm = torch.zeros((max(n2, 1), h.n_params), **f64)
+        h.run(n2, adapt=True, record={i: warm[i] for i in range(n2)})
+        h.end_adaptation()
+        if n2 >= 2:
+            h.adapt_mass_from(warm[:n2])
+        h.start_adaptation()
+        h.run(max(n_draws // 2, 1), adapt=True)
+        h.end_adaptation()
+        acc0 = h.accepted.clone()
+        draws = torch.zeros((max(n_draws, 1), h.n_params), **f64)
+        h.run(n_draws, record={i: draws[i] for i in range(n_draws)})
+        rate = ((h.accepted - acc0).double() / max(n_draws, 1)).cpu().numpy()
+        theta = (h.lower + (h.upper - h.lower) * torch.sigmoid(draws[:n_draws])).cpu().numpy()
+        out = []
+        for i, (t, p) in enumerate(zip(tasks, patches)):
+            th = theta[:, h.slices[i]]
+            ns = int(p.n_sources)
+            npar = p.n_bands + 6
+            mean = th.mean(axis=0).reshape(ns, npar)
+            final = t["active"].copy()
+            ra0, dec0 = p.patch_reference_coordinates
+            for j, b in enumerate(p.bandlist):
+                final[b] = mean[:, j]
+            for j, c in enumerate(t["shape_cols"]):
+                final[c] = mean[:, p.n_bands + j]
+            final["ra"] += ra0
+            final["dec"] += dec0
+            covs = None
+            if list(p.bandlist) == list(t["bands"]) and n_draws >= 2:
+                blocks = th.reshape(n_draws, ns, npar)
+                covs = np.stack([np.cov(blocks[:, k, :], rowvar=False) for k in range(ns)])
+            out.append(dict(final=final, covs=covs, niter=n_draws, acceptance=float(rate[i])))
+        for p in patches:
+            p.free()
         return out
 
     return work

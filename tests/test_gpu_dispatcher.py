@@ -30,16 +30,9 @@ def _field(rng, n=12):
     return cat
 
 
-def test_flux_fit_rounds_on_a_fits_field(tmp_path):
-    from test_stores import _PSF, make_image_set
-    from forcepho_b200 import dispatcher as D
-    from forcepho_b200 import superscene as SS
-    from forcepho_b200.proposal import B200Proposer
+def _truth_patcher(paths, truth):
+    from test_stores import _PSF
     from forcepho_b200.stores.patch import FITSPatch
-
-    rng = np.random.default_rng(41)
-    paths = make_image_set(tmp_path, seed=9, size=(120, 96))
-    truth = _field(rng)
 
     class TruthPatch(FITSPatch):
         """Image noise plus the FP64 model of every true source."""
@@ -57,6 +50,65 @@ def test_flux_fit_rounds_on_a_fits_field(tmp_path):
         p.psfstore = _PSF()
         return p
 
+    return make_patcher
+
+
+def test_hmc_rounds_on_a_fits_field(tmp_path):
+    """The sampling work unit: every region of a round sampled together on
+    the device within its prior bounds; the posterior means move the fluxes
+    towards the truth and the scene counts the draws."""
+    from test_stores import make_image_set
+    from forcepho_b200 import dispatcher as D
+    from forcepho_b200 import superscene as SS
+
+    rng = np.random.default_rng(43)
+    paths = make_image_set(tmp_path, seed=11, size=(120, 96))
+    truth = _field(rng)
+    cat = truth.copy()
+    for b in BANDS:
+        cat[b] *= rng.uniform(0.8, 1.2, len(cat))
+    start = cat.copy()
+    scene = SS.SuperScene(sourcecat=cat, bands=BANDS, maxactive_per_patch=4, maxradius=0.6, boundary_radius=0.8,
+                          nscale=3, minradius=0.15, target_niter=20, maxactive_fraction=0.9,
+                          rng=np.random.default_rng(6))
+    results = []
+    work = D.hmc_work(_truth_patcher(paths, truth), BANDS, n_warmup=20, n_draws=20, n_steps=8, seed=3,
+                      tile_pixels=256)
+
+    def logged(tasks):
+        res = work(tasks)
+        results.extend(res)
+        return res
+
+    rounds = D.run(scene, logged, batch_per_rank=4, max_rounds=2)
+    assert rounds and len(results) == sum(r["tasks"] for r in rounds)
+    for r in results:
+        assert 0.2 < r["acceptance"] <= 1.0, r["acceptance"]
+        for c in BANDS + ["ra", "dec", "q", "pa", "sersic", "rhalf"]:
+            assert np.all(np.isfinite(r["final"][c]))
+        if r["covs"] is not None:
+            assert r["covs"].shape == (len(r["final"]), 8, 8)
+            assert np.all(np.linalg.eigvalsh(r["covs"]) > -1e-12)
+    done = scene.sourcecat["n_iter"] >= 20
+    assert done.sum() >= 2
+    SS.check_bounds(scene.sourcecat[done], scene.bounds_catalog[done])
+    for b in BANDS:
+        err0 = np.abs(start[b][done] - truth[b][done])
+        err1 = np.abs(scene.sourcecat[b][done] - truth[b][done])
+        assert np.median(err1) < np.median(err0)
+
+
+def test_flux_fit_rounds_on_a_fits_field(tmp_path):
+    from test_stores import make_image_set
+    from forcepho_b200 import dispatcher as D
+    from forcepho_b200 import superscene as SS
+    from forcepho_b200.proposal import B200Proposer
+
+    rng = np.random.default_rng(41)
+    paths = make_image_set(tmp_path, seed=9, size=(120, 96))
+    truth = _field(rng)
+
+    make_patcher = _truth_patcher(paths, truth)
     cat = truth.copy()
     for b in BANDS:
         cat[b] *= rng.uniform(0.7, 1.3, len(cat))       # starting fluxes off the truth
