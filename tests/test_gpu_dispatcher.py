@@ -66,9 +66,9 @@ def test_hmc_rounds_on_a_fits_field(tmp_path):
     rng = np.random.default_rng(43)
     paths = make_image_set(tmp_path, seed=11, size=(120, 96))
     truth = _field(rng)
+    # the catalog starts at the truth: fixed sources are then subtracted
+    # exactly, and the posterior of the active ones must contain the truth
     cat = truth.copy()
-    for b in BANDS:
-        cat[b] *= rng.uniform(0.8, 1.2, len(cat))
     start = cat.copy()
     scene = SS.SuperScene(sourcecat=cat, bands=BANDS, maxactive_per_patch=4, maxradius=0.6, boundary_radius=0.8,
                           nscale=3, minradius=0.15, target_niter=40, maxactive_fraction=0.9,
