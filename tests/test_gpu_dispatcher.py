@@ -73,6 +73,13 @@ def test_hmc_rounds_on_a_fits_field(tmp_path):
     scene = SS.SuperScene(sourcecat=cat, bands=BANDS, maxactive_per_patch=4, maxradius=0.6, boundary_radius=0.8,
                           nscale=3, minradius=0.15, target_niter=40, maxactive_fraction=0.9,
                           rng=np.random.default_rng(6))
+    # narrow shape priors around the truth: the flux posterior is then nearly
+    # Gaussian and 40 draws sample it well (with free shapes, flux and size
+    # trade off and a short chain understates the width along that direction)
+    bc = scene.bounds_catalog
+    for c, h in (("q", 0.02), ("pa", 0.05), ("sersic", 0.05), ("rhalf", 0.005)):
+        bc[c][:, 0] = truth[c] - h
+        bc[c][:, 1] = truth[c] + h
     results = []
     work = D.hmc_work(_truth_patcher(paths, truth), BANDS, n_warmup=40, n_draws=40, n_steps=8, seed=3,
                       tile_pixels=256)
@@ -104,7 +111,7 @@ def test_hmc_rounds_on_a_fits_field(tmp_path):
             for j, b in enumerate(BANDS):
                 z.append(abs(r["final"][b][k] - truth[b][i]) / sd[k, j])
     z = np.array(z)
-    assert np.all(z < 5) and np.median(z) < 2.5, z
+    assert np.all(z < 5) and np.median(z) < 2.0, z
     assert not np.array_equal(scene.sourcecat[BANDS[0]][done], start[BANDS[0]][done])
 
 
