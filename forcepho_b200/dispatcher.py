@@ -62,7 +62,10 @@ def run(scene, work, batch_per_rank=8, rank=0, world=1, group=None, ntry=1000, m
     ``work(tasks)`` returns one result dict per task with ``final`` (the
     active rows with new parameters) and optionally ``niter`` (default 1)
     and ``covs``.  Every rank calls this; returns per-round records on rank 0
-    (rounds, tasks, seconds) and None elsewhere."""
+    (rounds, tasks, seconds) and None elsewhere.  An exception in ``work`` on
+    one rank ends that rank's call; the others then fail in the round's
+    ``gather_object`` when the process group's timeout runs out, so give the
+    group a short timeout."""
     import torch.distributed as dist
     distributed = world > 1
     rounds, taskid = [], 0
@@ -193,6 +196,8 @@ def hmc_work(make_patcher, allbands, n_warmup=40, n_draws=40, n_steps=16, seed=0
     import torch
     from .hmc import DeviceHMC
     from .superscene import bounds_vectors
+    if n_draws < 1 or n_warmup < 0 or n_steps < 1:
+        raise ValueError("hmc_work needs n_draws >= 1, n_warmup >= 0 and n_steps >= 1")
 
     def work(tasks):
         patches, scenes, theta0, bounds = [], [], [], []

@@ -136,7 +136,7 @@ class SuperScene:
     # --- state ---
     @property
     def sparse(self):
-        return self.n_active * 1.0 / self.n_sources < self.maxactive_fraction
+        return self.n_sources > 0 and self.n_active * 1.0 / self.n_sources < self.maxactive_fraction
 
     @property
     def undone(self):
@@ -182,7 +182,11 @@ class SuperScene:
     def scene_center(self):
         """(ra, dec) degrees of the scene frame's origin: the catalog's median position."""
         if "_scene_center" not in self.__dict__:
-            self._scene_center = (float(np.median(self.sourcecat["ra"])), float(np.median(self.sourcecat["dec"])))
+            if self.n_sources == 0:
+                self._scene_center = (0.0, 0.0)
+            else:
+                self._scene_center = (float(np.median(self.sourcecat["ra"])),
+                                      float(np.median(self.sourcecat["dec"])))
         return self._scene_center
 
     def sky_to_scene(self, ra, dec):
@@ -554,6 +558,8 @@ def flux_bounds(flux, unc1, snr_max=10, precisions=None):
     half-width of |flux| / (sqrt|flux| / unc1), widened to at least
     (unc1/2)^2 on each side of faint fluxes; non-finite bounds replaced."""
     flux = np.asarray(flux, dtype=np.float64)
+    if flux.size == 0:
+        return flux.copy(), flux.copy()
     if precisions is not None:
         sigma = np.maximum(np.sqrt(np.diag(np.linalg.pinv(precisions))), flux / snr_max)
         lo = flux - unc1 * sigma

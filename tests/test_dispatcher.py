@@ -106,3 +106,12 @@ def test_two_ranks_match_one_process(tmp_path):
     s0, s1 = np.load(tmp_path / "seen0.npy"), np.load(tmp_path / "seen1.npy")
     assert len(s0) and len(s1)                                   # both ranks worked
     assert sorted(np.concatenate([s0, s1]).tolist()) == list(range(sum(r["tasks"] for r in want)))
+
+
+def test_empty_scene_and_bad_sampling_arguments():
+    cat = np.zeros(0, dtype=SS.sourcecat_dtype(bands=["B0"]))
+    sc = SS.SuperScene(sourcecat=cat, bands=["B0"])
+    assert not sc.sparse and D.checkout_batch(sc, 4) == []
+    assert D.run(sc, D.dummy_work, batch_per_rank=2) == []
+    with pytest.raises(ValueError):
+        D.hmc_work(lambda: None, ["B0"], n_draws=0)
