@@ -115,3 +115,40 @@ def test_empty_scene_and_bad_sampling_arguments():
     assert D.run(sc, D.dummy_work, batch_per_rank=2) == []
     with pytest.raises(ValueError):
         D.hmc_work(lambda: None, ["B0"], n_draws=0)
+
+
+def _failing_worker(rank, world, port, outdir):
+    import datetime
+    import sys
+    import torch.distributed as dist
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=10))
+    sc = _scene() if rank == 0 else None
+
+    def work(tasks):
+        if rank == 1:
+            raise RuntimeError("work failed on rank 1")
+        return _checked_work(tasks)
+
+    try:
+        D.run(sc, work, batch_per_rank=2, rank=rank, world=world, max_rounds=3)
+        outcome = "finished"
+    except Exception as e:                      # noqa: BLE001 -- recorded for the test
+        outcome = "%s: %s" % (type(e).__name__, str(e)[:200])
+    with open(os.path.join(outdir, "outcome%d.txt" % rank), "w") as f:
+        f.write(outcome)
+    dist.destroy_process_group()
+
+
+@pytest.mark.timeout(180)
+def test_a_failing_rank_ends_the_run_on_every_rank(tmp_path):
+    """A work unit that raises on one rank: that rank leaves the round, and
+    rank 0 gets an error from the round's gather (the peer is gone, or the
+    process group's 10 s timeout runs out) instead of waiting for ever."""
+    import torch.multiprocessing as mp
+    mp.spawn(_failing_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
+    out0 = (tmp_path / "outcome0.txt").read_text()
+    out1 = (tmp_path / "outcome1.txt").read_text()
+    assert out1.startswith("RuntimeError: work failed on rank 1")
+    assert out0 != "finished", out0
