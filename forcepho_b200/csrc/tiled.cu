@@ -64,6 +64,7 @@ static_assert(FP_RUN == 32, "the forward pass sums runs of one 32-Gaussian ballo
 // about one FP32 rounding, whatever the number of terms.  Used by the FP32 +
 // Kahan precision variant (FP_KAHAN); the normal build flushes FP32 runs into
 // FP64 instead.
+#ifdef FP_KAHAN
 __device__ __forceinline__ void kahan_add(float &s, float &c, float x)
 {
     const float y = x - c;
@@ -71,6 +72,7 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x)
     c = (t - s) - y;
     s = t;
 }
+#endif
 
 // A chunk's last group of v < 32 Gaussians is replicated min(8, 32 / v) times
 // across the warp's lanes in the adjoint, each replica taking every k-th pixel;
