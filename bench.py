@@ -1030,6 +1030,50 @@ def run_precision(args):
         p.free()
     print(json.dumps({"metric": "error vs FP64 oracle", "variant": variant, "library": N.lib_path(),
                       "worst": worst, "cases": rows}), flush=True)
+    print(json.dumps(precision_full(args, variant)), flush=True)
+
+
+def precision_full(args, variant):
+    """The whole batched workload (every patch, the bench's proposals) through
+    the batched FP32 path, against the device FP64 evaluation
+    (fp_evaluate_proposal_f64, itself held to the FP64 oracle at 1e-11 by the
+    tests).  Raw chi2 error per band uses the band scale sum (r^2 + d^2) ierr^2
+    = chi2_f64 + 2 sum d^2 ierr^2."""
+    import torch
+    from forcepho_b200.batch import BatchedProposer
+    from forcepho_b200.proposal import F64Proposer
+    patches = make_patches(argparse.Namespace(**{**vars(args), "workload": "batched"}), 0)
+    for p in patches:
+        p.return_residual = False
+        p.send_to_device()
+    proposals = perturbed_proposals(patches)
+    bp = BatchedProposer(patches, tile_pixels=args.tile_pixels or 1024, autotune=False)
+    got = bp.evaluate_proposals(proposals)
+    f64 = F64Proposer()
+    t0 = time.perf_counter()
+    worst = {"chi2_relerr": 0.0, "grad_norm": 0.0, "grad_comp_max": 0.0}
+    where = {}
+    for i, (p, prop) in enumerate(zip(patches, proposals)):
+        c64, g64 = f64.evaluate_proposal(prop, patch=p)
+        c32, g32 = got[i]
+        for b in range(p.n_bands):
+            e0, ne = int(p.band_start[b]), int(p.band_N[b])
+            s0 = int(p.exposure_start[e0])
+            s1 = int(p.exposure_start[e0 + ne - 1] + p.exposure_N[e0 + ne - 1])
+            d = p.data[s0:s1].astype(np.float64) * p.ierr[s0:s1]
+            sc = c64[b] + 2.0 * float(np.sum(d * d))
+            e = abs(c32[b] - c64[b]) / max(abs(c64[b]), RAW_FLOOR * sc)
+            if e > worst["chi2_relerr"]:
+                worst["chi2_relerr"], where["chi2_relerr"] = e, i
+        for c in component_errors(g32, g64):
+            for k in ("norm", "comp_max"):
+                key = "grad_" + k
+                if c[k] > worst[key]:
+                    worst[key], where[key] = c[k], i
+    torch.cuda.synchronize()
+    return {"metric": "error vs device FP64 (whole workload)", "variant": variant, "workload": "batched",
+            "patches": len(patches), "pairs": int(bp.n_pairs), "worst": worst, "worst_patch": where,
+            "f64_seconds": time.perf_counter() - t0}
 
 
 def main():

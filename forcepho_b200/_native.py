@@ -99,6 +99,9 @@ SIGNATURES = {
     "fp_struct_sizes": (ctypes.c_int, [c_vp]),
     "fp_evaluate_proposal_plain": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp]),
     "fp_evaluate_proposal": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp]),
+    "fp_f64_workspace_bytes": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(c_sz)]),
+    "fp_evaluate_proposal_f64": (ctypes.c_int, [c_vp, c_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, c_vp, c_vp,
+                                                c_vp, c_sz, c_vp]),
     "fp_evaluate_proposal_release": (ctypes.c_int, []),
     "fp_plan_count": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(PlanSizes)]),
     "fp_plan_fill": (ctypes.c_int, [c_vp, ctypes.c_int, ctypes.c_int, c_vp, c_vp, c_vp, c_vp, c_vp]),

@@ -13,7 +13,9 @@ that has been ``send_to_device``-ed, and returns
 
 It runs the tiled sm_100a kernels through the C ABI (``fp_evaluate_batch`` with
 one patch).  ``PlainProposer`` has the same surface over the one-CTA-per-band
-comparator kernel (``fp_evaluate_proposal_plain``).  ``Proposer`` is an alias
+comparator kernel (``fp_evaluate_proposal_plain``), and ``F64Proposer`` the
+FP64 device evaluation (``fp_evaluate_proposal_f64``, a precision reference
+without residuals).  ``Proposer`` is an alias
 of ``B200Proposer``, as ``Proposer`` aliases ``GPUProposer`` in the reference.
 """
 
@@ -28,7 +30,7 @@ from .device import Plan, current_stream_ptr, response_view
 from .kernel_limits import MAXBANDS, MAXRADII, MAXSOURCES, NPARAMS
 from .structs import response_struct_dtype, source_struct_dtype
 
-__all__ = ["ProposerBase", "B200Proposer", "PlainProposer", "Proposer",
+__all__ = ["ProposerBase", "B200Proposer", "PlainProposer", "F64Proposer", "Proposer",
            "source_struct_dtype", "response_struct_dtype", "MAXBANDS", "MAXRADII", "MAXSOURCES", "NPARAMS"]
 
 
@@ -163,6 +165,61 @@ class B200Proposer(ProposerBase):
             self._queue(plan, lp)
         torch.cuda.synchronize()
         self._graph = g
+
+
+class F64Proposer(ProposerBase):
+    """The likelihood and gradient of one proposal in FP64 on the device
+    (``fp_evaluate_proposal_f64``): a precision reference for whole patches,
+    where the CPU oracle is too slow.  ``evaluate_proposal`` returns
+
+    * ``chi2``        float64[n_bands]
+    * ``chi2_derivs`` float64[n_bands, n_sources, 7], same order as the
+      Response records.
+
+    No residual is written and nothing is culled; a patch whose exposures
+    hold more Gaussians than the plan raises ``RuntimeError``.
+    """
+
+    def __init__(self, patch=None):
+        self.L = N.load()
+        self.patch = patch
+        self._ws = None
+
+    def _workspace(self, patch, max_gauss, device):
+        n = ctypes.c_size_t()
+        N.check(self.L.fp_f64_workspace_bytes(patch.n_exp, max_gauss, ctypes.byref(n)), "fp_f64_workspace_bytes")
+        if self._ws is None or self._ws.numel() < n.value or self._ws.device != device:
+            self._ws = torch.zeros(n.value, dtype=torch.uint8, device=device)
+        return self._ws, n.value
+
+    def evaluate_proposal(self, proposal, patch=None, verbose=False, unpack=True):
+        if patch is None:
+            patch = self.patch
+        prop = self._check_proposal(proposal, patch)
+        device = patch.device_patch.device
+        n_bands, n_sources = patch.n_bands, int(patch.n_sources)
+        max_gauss = patch.max_gauss_per_exposure()
+        ws, nbytes = self._workspace(patch, max_gauss, device)
+        host = np.zeros(max(len(prop), 1), dtype=source_struct_dtype)
+        host[:len(prop)] = prop
+        d_prop = torch.from_numpy(host.view(np.uint8).copy()).to(device)
+        chi2 = torch.zeros(MAXBANDS, dtype=torch.float64, device=device)
+        dchi2 = torch.zeros((MAXBANDS, MAXSOURCES, NPARAMS), dtype=torch.float64, device=device)
+        stream = torch.cuda.current_stream()
+        if verbose:
+            print("Launching FP64 evaluation over %d exposures" % patch.n_exp, file=sys.stderr, flush=True)
+        N.check(self.L.fp_evaluate_proposal_f64(
+            ctypes.c_void_p(patch.device_patch_ptr), ctypes.c_void_p(d_prop.data_ptr()), n_bands, patch.n_exp,
+            max_gauss, ctypes.c_void_p(chi2.data_ptr()), ctypes.c_void_p(dchi2.data_ptr()),
+            ctypes.c_void_p(ws.data_ptr()), nbytes, current_stream_ptr(stream)), "fp_evaluate_proposal_f64")
+        st = ctypes.c_int32()
+        N.check(self.L.fp_read_status(ctypes.c_void_p(ws.data_ptr()), ctypes.byref(st), current_stream_ptr(stream)),
+                "fp_read_status")
+        if st.value:
+            raise RuntimeError("fp_evaluate_proposal_f64: device status %d" % st.value)
+        out_chi2 = chi2[:n_bands].cpu().numpy()
+        out_d = dchi2[:n_bands, :n_sources].cpu().numpy()
+        return out_chi2, out_d
 
 
 Proposer = B200Proposer

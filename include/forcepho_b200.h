@@ -164,6 +164,30 @@ FP_API int fp_evaluate_proposal_plain(const fp_patch *d_patch, const fp_source *
                                int n_bands, int max_gauss_per_exposure,
                                double *d_chi2, fp_response *d_response, void *stream);
 
+/* The same evaluation in FP64 on the device: image Gaussians, pixel models,
+ * residuals, chi2 and every gradient term in double precision, with the
+ * reference's formulas (compute_gaussians_kernel.cc:227-315) and its
+ * MAX_EXP_ARG skip.  A precision reference at full size: the FP32 paths are
+ * compared against it on whole workloads, where the CPU oracle would take
+ * hours.  Sums use FP64 atomics, so results are exact to about 1e-15 but not
+ * bitwise reproducible.
+ *
+ *   d_patch, d_proposal      as fp_evaluate_proposal_plain
+ *   n_bands, n_exposures     the patch's counts
+ *   max_gauss_per_exposure   n_sources * max_b n_psf_per_source[b]
+ *   d_chi2                   device f64[n_bands]
+ *   d_dchi2                  device f64[n_bands][MAXSOURCES * NPARAMS], source-major like
+ *                            fp_response (entries past n_sources are zero)
+ *   d_workspace              device buffer of fp_f64_workspace_bytes bytes, 256-byte aligned
+ * Queued on `stream`; an exposure with more Gaussians than max_gauss_per_exposure
+ * sets FP_STATUS_GAUSS_COUNT in the workspace's status word (fp_read_status on
+ * d_workspace) and contributes nothing. */
+FP_API int fp_f64_workspace_bytes(int n_exposures, int max_gauss_per_exposure, size_t *out);
+FP_API int fp_evaluate_proposal_f64(const fp_patch *d_patch, const fp_source *d_proposal, int n_bands,
+                                    int n_exposures, int max_gauss_per_exposure, double *d_chi2,
+                                    double *d_dchi2, void *d_workspace, size_t workspace_bytes,
+                                    void *stream);
+
 /* One proposal on one patch with the kernel ABI of the reference's
  * EvaluateProposal (forcepho/src/compute_gaussians_kernel.cu:212-214, launched
  * by GPUProposer.evaluate_proposal, forcepho/proposal.py:96-152): device patch

@@ -225,3 +225,28 @@ def test_planner_tile_rule_classes():
     bad = N.tile_rule([(4096, 256), (16384, 500)])
     assert L.fp_plan_count_rule(ctypes.addressof(arr), len(shapes), ctypes.byref(bad), ctypes.byref(sz)) \
         == N.FP_ERR_ARGUMENT
+
+
+def test_f64_entry_point_rejects_bad_arguments():
+    """fp_evaluate_proposal_f64 checks its arguments on the host, before any
+    CUDA call: the pointers here are never dereferenced."""
+    import ctypes
+    from forcepho_b200 import _native as N
+    from forcepho_b200.kernel_limits import MAXBANDS
+    L = N.load()
+    n = ctypes.c_size_t()
+    assert L.fp_f64_workspace_bytes(3, 40, ctypes.byref(n)) == N.FP_OK
+    assert n.value >= 256 + 3 * 40 and n.value % 256 == 0
+    assert L.fp_f64_workspace_bytes(-1, 40, ctypes.byref(n)) == N.FP_ERR_ARGUMENT
+    fake, ws = ctypes.c_void_p(4096), ctypes.c_void_p(8192)
+
+    def call(n_bands=2, n_exp=3, ws_ptr=ws, ws_bytes=n.value):
+        return L.fp_evaluate_proposal_f64(fake, fake, n_bands, n_exp, 40, fake, fake, ws_ptr, ws_bytes, None)
+
+    assert L.fp_f64_workspace_bytes(3, 40, ctypes.byref(n)) == N.FP_OK
+    assert call(n_bands=0) == N.FP_ERR_LIMITS
+    assert call(n_bands=MAXBANDS + 1) == N.FP_ERR_LIMITS
+    assert call(ws_ptr=ctypes.c_void_p(8192 + 16)) == N.FP_ERR_ARGUMENT
+    assert call(ws_bytes=n.value - 1) == N.FP_ERR_WORKSPACE
+    assert b"workspace" in L.fp_error_string()
+    assert L.fp_evaluate_proposal_f64(None, fake, 2, 3, 40, fake, fake, ws, n.value, None) == N.FP_ERR_ARGUMENT
