@@ -47,7 +47,8 @@ def test_multiband_workload_in_fp64(golden_multiband):
     p = _device(p)
     for k in (0, 1):
         chi2, dchi2 = F64Proposer(p).evaluate_proposal(g[f"proposal_{k}"])
-        sc = band_scales(p, g[f"f64_residual_{k}"])
+        # sum (r^2 + d^2) ierr^2 = chi2 + 2 sum d^2 ierr^2 (the fixture keeps no residual)
+        sc = g[f"f64_chi2_{k}"] + 2.0 * band_scales(p, np.zeros(p.npix))
         assert chi2_raw_err(chi2, g[f"f64_chi2_{k}"], sc) < CHI2_EXACT
         assert grad_err(dchi2, g[f"f64_dchi2_{k}"]) < GRAD_EXACT
 
