@@ -116,7 +116,7 @@ def test_gaussian_count_over_the_plan_sets_the_status():
     assert st.value == N.STATUS_GAUSS_COUNT
     # outputs were cleared and nothing was added for the rejected exposures
     assert torch.all(chi2[:p.n_bands] == 0) and torch.all(dchi2[:p.n_bands] == 0)
-    # the status word was cleared by the read; a sized call leaves it clear
+    # the status word was cleared by the read; a sized call evaluates every band
     from forcepho_b200.proposal import F64Proposer
     c, _ = F64Proposer().evaluate_proposal(prop, patch=p)
-    assert np.all(c > 0)
+    assert np.all(c != 0)
