@@ -43,6 +43,7 @@ EX2_PER_PAIR = 2
 # raw chi2 errors of a band are measured against max(|chi2|, RAW_FLOOR * the
 # band's sum (r^2 + d^2) ierr^2), as the parity tests measure them
 RAW_FLOOR = 1e-2
+PARAM_NAMES = ["flux", "ra", "dec", "q", "pa", "sersic", "rhalf"]
 
 
 # DRAM bytes (read + write) of one tile_kernel launch, measured by ncu
@@ -1023,7 +1024,7 @@ def run_precision(args):
         ce = [abs(chi2[b] - c64[b]) / max(abs(c64[b]), RAW_FLOOR * s_) for b, s_ in zip(bl, sc)]
         cols = component_errors(dchi2[bl], g64[bl])
         rows.append({"patch": name, "pairs": int(p.n_pairs()), "bands": bl, "chi2_relerr": ce,
-                     "grad": dict(zip(["flux", "ra", "dec", "q", "pa", "sersic", "rhalf"], cols))})
+                     "grad": dict(zip(PARAM_NAMES, cols))})
         worst["chi2_relerr"] = max(worst["chi2_relerr"], max(ce))
         worst["grad_norm"] = max(worst["grad_norm"], max(c["norm"] for c in cols))
         worst["grad_comp_max"] = max(worst["grad_comp_max"], max(c["comp_max"] for c in cols))
@@ -1064,12 +1065,12 @@ def precision_full(args, variant):
             sc = c64[b] + 2.0 * float(np.sum(d * d))
             e = abs(c32[b] - c64[b]) / max(abs(c64[b]), RAW_FLOOR * sc)
             if e > worst["chi2_relerr"]:
-                worst["chi2_relerr"], where["chi2_relerr"] = e, i
-        for c in component_errors(g32, g64):
+                worst["chi2_relerr"], where["chi2_relerr"] = e, [i, b]
+        for name, c in zip(PARAM_NAMES, component_errors(g32, g64)):
             for k in ("norm", "comp_max"):
                 key = "grad_" + k
                 if c[k] > worst[key]:
-                    worst[key], where[key] = c[k], i
+                    worst[key], where[key] = c[k], [i, name]
     torch.cuda.synchronize()
     return {"metric": "error vs device FP64 (whole workload)", "variant": variant, "workload": "batched",
             "patches": len(patches), "pairs": int(bp.n_pairs), "worst": worst, "worst_patch": where,

@@ -120,3 +120,47 @@ def test_gaussian_count_over_the_plan_sets_the_status():
     from forcepho_b200.proposal import F64Proposer
     c, _ = F64Proposer().evaluate_proposal(prop, patch=p)
     assert np.all(c != 0)
+
+
+@pytest.mark.timeout(900)
+def test_whole_batched_workload_against_fp64():
+    """Full-size parity: all 512 patches of the batched workload (1.04e11
+    pixel-Gaussian pairs), evaluated by the batched FP32 path in one launch
+    set, against the device FP64 evaluation patch by patch, with the FP64
+    tolerances of the parity tests.  Raw chi2 per band is measured against
+    max(|chi2|, RAW_FLOOR sum (r^2 + d^2) ierr^2), where sum (r^2 + d^2) ierr^2
+    = chi2_f64 + 2 sum d^2 ierr^2."""
+    from forcepho_b200 import synthetic as S
+    from forcepho_b200.batch import BatchedProposer, render_models
+    from forcepho_b200.proposal import F64Proposer
+    patches = []
+    for sh in S.batched_shapes(seed=4, n_patches=512):
+        rng = np.random.default_rng(sh["seed"])
+        p = S.make_patch(rng, n_sources=sh["n_sources"], exp_per_band=sh["exp_per_band"], exp_pix=sh["exp_pix"],
+                         n_psf=4, source_params=S._broad_source, raster_width=256)
+        p._rng = rng
+        patches.append(p)
+    sigmas = [p._rng.uniform(0.5, 2.0, p.n_exp) for p in patches]
+    for p, m, sg in zip(patches, render_models(patches), sigmas):
+        S.add_noise(p, p._rng, sg, m)
+        _device(p)
+    rng = np.random.default_rng(99)
+    proposals = []
+    for p in patches:
+        q = p.scene.get_proposal().copy()
+        q["ra"] += rng.normal(0, 2e-6, len(q)).astype(np.float32)
+        q["dec"] += rng.normal(0, 2e-6, len(q)).astype(np.float32)
+        q["q"] = np.clip(q["q"] * rng.uniform(0.95, 1.05, len(q)), 0.2, 0.99).astype(np.float32)
+        proposals.append(q)
+    got = BatchedProposer(patches, tile_pixels=1024, autotune=False).evaluate_proposals(proposals)
+    f64 = F64Proposer()
+    worst_c, worst_g = 0.0, 0.0
+    for i, (p, q) in enumerate(zip(patches, proposals)):
+        c64, g64 = f64.evaluate_proposal(q, patch=p)
+        c32, g32 = got[i]
+        sc = c64 + 2.0 * band_scales(p, np.zeros(p.npix))
+        worst_c = max(worst_c, chi2_raw_err(c32, c64, sc))
+        worst_g = max(worst_g, grad_err(g32, g64))
+        p.free()
+    assert worst_c < CHI2_F64, worst_c
+    assert worst_g < GRAD_F64, worst_g
