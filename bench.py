@@ -14,7 +14,10 @@ with CUDA events); ``e2e`` = the same through ``BatchedProposer.evaluate_proposa
 with host proposals in and chi2/gradients out every step; ``plain`` = the
 one-launch-per-patch port-equivalent kernel on the same patches;
 ``roofline`` = the tile kernel's FP32 work against the FP32 peak measured in
-this run; ``cpu_baseline`` = the reference CPU kernel on a bounded sample.
+this run; ``cpu_baseline`` = the reference CPU kernel on a bounded sample;
+``precision`` = errors against the FP64 oracle and the reference kernel on a
+sample of patches, and of every patch of the batch against the device FP64
+evaluation.
 
 ``--impl reference`` times the reference's own CPU kernel
 (forcepho/src/compute_gaussians_kernel.cc built from source in oracle/_ref)
