@@ -111,8 +111,11 @@ class PatchFarm:
 # ---------------------------------------------------------------------------
 # attributes of a patch that belong to its device copy, not to its arrays
 _DEVICE_STATE = ("device_ptrs", "device_patch", "patch_struct", "device_generation", "data_generation")
-# per-exposure lists and arrays some patch classes carry besides the kernel's
-_PER_EXPOSURE = ("psf_blocks", "original_shapes", "original_sizes", "sigma")
+# per-exposure lists and arrays some patch classes carry besides the kernel's:
+# synthetic patches (PSF blocks, stamp shapes, noise levels) and store-backed
+# ones (headers, WCS, exposure paths, band names, background offsets)
+_PER_EXPOSURE = ("psf_blocks", "original_shapes", "original_sizes", "sigma", "hdrs", "wcses", "epaths", "bands",
+                 "background_offsets")
 
 
 def _band_of_exposure(patch):
@@ -169,6 +172,8 @@ def exposure_subpatch(patch, exposures):
         v = getattr(patch, name, None)
         if v is not None and len(v) == ne:
             setattr(sub, name, [v[e] for e in ex] if isinstance(v, list) else np.asarray(v)[ex])
+    if getattr(patch, "n_exp_per_band", None) is not None:
+        sub.n_exp_per_band = np.asarray(sub.band_N).astype(np.asarray(patch.n_exp_per_band).dtype)
     ast = getattr(patch, "astrometry", None)
     if isinstance(ast, tuple) and all(len(a) == ne for a in ast):
         sub.astrometry = tuple(np.asarray(a)[ex] for a in ast)

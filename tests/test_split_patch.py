@@ -123,3 +123,34 @@ def test_two_gloo_ranks_share_one_patch(tmp_path):
             # the ranks' FP32 gradients summed in FP64 and rounded once
             assert np.linalg.norm(g[..., k] - g_all[..., k]) <= 1e-6 * np.linalg.norm(g_all[..., k])
     np.testing.assert_array_equal(np.load(tmp_path / "c0.npy"), np.load(tmp_path / "c1.npy"))
+
+
+def test_store_patch_subpatch_repacks_its_own_metadata(tmp_path):
+    """A sub-patch of a FITS-backed patch keeps its exposures' WCS, headers
+    and band names, so repacking the scene's metadata on it gives the rows
+    of the whole patch's metadata for those exposures; the partition sums
+    hold as for synthetic patches."""
+    from test_stores import _PSF, make_image_set
+    from forcepho_b200.stores.patch import FITSPatch
+    from forcepho_b200.stores.region import CircularRegion
+    paths = make_image_set(tmp_path, seed=9, n_exp=(2, 2))
+    p = FITSPatch(fitsfiles=paths)
+    p.psfstore = _PSF()
+    cat = np.zeros(2, dtype=[(c, np.float64) for c in ("ra", "dec", "q", "pa", "sersic", "rhalf", "B0", "B1")])
+    cat["ra"] = [53.1, 53.1 + 5e-5]
+    cat["dec"] = [-27.8, -27.8 - 3e-5]
+    cat["q"], cat["pa"], cat["sersic"], cat["rhalf"] = [0.8, 0.6], [0.3, -0.5], [2.0, 1.5], [0.1, 0.2]
+    cat["B0"], cat["B1"] = [10.0, 5.0], [7.0, 3.0]
+    p.build_patch(CircularRegion(53.1, -27.8, 0.6 / 3600.0), cat, allbands=["B0", "B1"])
+    prop = p.scene.get_proposal()
+    c_all, g_all, _ = O.evaluate(p, prop, precision="f64")
+    sub = D.exposure_subpatch(p, [1, 2])
+    assert list(sub.band_N) == [1, 1] and list(sub.n_exp_per_band) == [1, 1]
+    assert sub.bands == [p.bands[1], p.bands[2]] and sub.wcses == [p.wcses[1], p.wcses[2]]
+    meta = sub.meta_for(sub.scene)
+    for name in ("D", "CW", "crpix", "crval"):
+        np.testing.assert_allclose(meta[name], getattr(p, name)[[1, 2]], rtol=0, atol=0, err_msg=name)
+    np.testing.assert_array_equal(meta["psfgauss"], sub.psfgauss)
+    rest = D.exposure_subpatch(p, [0, 3])
+    c = O.evaluate(sub, prop, precision="f64")[0] + O.evaluate(rest, prop, precision="f64")[0]
+    assert np.allclose(c, c_all, rtol=1e-12, atol=0)
