@@ -27,6 +27,8 @@ scene evolves identically for any number of ranks with the same total batch.
 
 import time
 
+import numpy as np
+
 from .distributed import balance
 
 __all__ = ["checkout_batch", "task_weight", "run", "dummy_work", "flux_fit_work", "hmc_work"]
@@ -35,10 +37,14 @@ __all__ = ["checkout_batch", "task_weight", "run", "dummy_work", "flux_fit_work"
 def checkout_batch(scene, n_max, ntry=1000, first_taskid=0):
     """Up to ``n_max`` regions checked out of ``scene``: for each, up to
     ``ntry`` seed draws until one gives a region; stops early when a region
-    cannot be found or the scene is no longer sparse.  Returns task dicts
+    cannot be found, the scene is no longer sparse or no source is left to
+    seed a region.  Returns task dicts
     (taskid, region, active, fixed, bounds, cov, bands, shape_cols)."""
     tasks = []
     while len(tasks) < n_max and scene.sparse:
+        w = scene.seed_weight()
+        if not (len(w) and np.all(np.isfinite(w)) and w.sum() > 0):
+            break                               # every source is checked out
         for _ in range(ntry):
             region, active, fixed = scene.checkout_region()
             if active is not None:
@@ -192,7 +198,6 @@ def hmc_work(make_patcher, allbands, n_warmup=40, n_draws=40, n_steps=16, seed=0
     active rows at the posterior mean), ``covs`` (per-source covariance of
     the draws when the patch has every scene band), ``niter`` = n_draws, and
     the acceptance rate of every patch."""
-    import numpy as np
     import torch
     from .hmc import DeviceHMC
     from .superscene import bounds_vectors

@@ -207,7 +207,10 @@ class SuperScene:
         0) and copies of its active and fixed catalog rows; those sources are
         marked unavailable.  Returns (center, None, None) when the region
         would contain an active source."""
-        cra, cdec = self.draw_center(seed_index=seed_index)
+        seed = self.draw_center(seed_index=seed_index)
+        if seed is None:
+            return None, None, None
+        cra, cdec = seed
         center = self.sky_to_scene(cra, cdec)
         radius, active_inds, fixed_inds = self.get_circular_scene(center)
         if radius is None:
@@ -293,10 +296,20 @@ class SuperScene:
             fixed_inds = others[:1]
         return radius, kinds[active_inds], kinds[fixed_inds]
 
+    def draw_seed(self):
+        """A random source index drawn with ``seed_weight`` probabilities, or
+        -1 when no source has weight (every source checked out)."""
+        w = self.seed_weight()
+        if self.n_sources == 0 or not np.all(np.isfinite(w)) or w.sum() <= 0:
+            return -1
+        return int(self.rng.choice(self.n_sources, p=w))
+
     def draw_center(self, seed_index=-1):
         """(ra, dec) of the seed source: ``seed_index`` if >= 0, else a random
-        draw with ``seed_weight`` probabilities."""
-        k = seed_index if seed_index >= 0 else self.rng.choice(self.n_sources, p=self.seed_weight())
+        draw (``draw_seed``); None when there is nothing to draw."""
+        k = seed_index if seed_index >= 0 else self.draw_seed()
+        if k < 0:
+            return None
         seed = self.sourcecat[k]
         return seed["ra"], seed["dec"]
 
@@ -307,8 +320,10 @@ class SuperScene:
         """Valid sources, down-weighted by exp(-(n_iter - mean n_iter) / 20)."""
         w = (self.sourcecat["is_valid"] != 0).astype(np.float64)
         n = np.abs(self.sourcecat["n_iter"]).astype(np.float64)
-        w *= np.exp((n.mean() - n) / 20.0)
-        return w / w.sum()
+        if len(n):
+            w *= np.exp((n.mean() - n) / 20.0)
+        t = w.sum()
+        return w / t if t > 0 else w
 
     def sigmoid_weight(self):
         """Inactive sources, weighted by a sigmoid of 1 - n_iter / target_niter."""
@@ -316,7 +331,8 @@ class SuperScene:
         a, b = 20., -1.0
         x = a * (1 - self.sourcecat["n_iter"] / self.target_niter) + b
         w *= 1 / (1 + np.exp(-x))
-        return w / w.sum()
+        t = w.sum()
+        return w / t if t > 0 else w
 
 
 class LinkedSuperScene(SuperScene):
@@ -393,7 +409,9 @@ class LinkedSuperScene(SuperScene):
         ((seed position, seed_index), None, None) when the seed's
         neighbourhood holds an active source."""
         if seed_index < 0:
-            seed_index = int(self.rng.choice(self.n_sources, p=self.seed_weight()))
+            seed_index = self.draw_seed()
+            if seed_index < 0:
+                return (None, -1), None, None
         region, active_inds, fixed_inds = self.grow_scene(seed_index, max_fixed)
         if active_inds is None:
             return (region, seed_index), None, None

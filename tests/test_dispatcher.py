@@ -152,3 +152,22 @@ def test_a_failing_rank_ends_the_run_on_every_rank(tmp_path):
     out1 = (tmp_path / "outcome1.txt").read_text()
     assert out1.startswith("RuntimeError: work failed on rank 1")
     assert out0 != "finished", out0
+
+
+def test_checkout_stops_when_every_source_is_taken():
+    """Three isolated sources in a scene that stays sparse: three regions of
+    one active source each, then nothing is left to seed a region, and
+    checkout ends quietly instead of failing on zero seed weights."""
+    bands = ["B0"]
+    for cls in (SS.SuperScene, SS.LinkedSuperScene):
+        cat = np.zeros(3, dtype=SS.sourcecat_dtype(bands=bands))
+        cat["ra"] = 53.1 + np.array([0.0, 0.01, 0.02])          # 36 arcsec apart
+        cat["dec"] = -27.8
+        cat["rhalf"], cat["roi"], cat["q"], cat["sersic"], cat["B0"] = 0.1, 0.3, 0.8, 2.0, 1.0
+        sc = cls(sourcecat=cat, bands=bands, maxactive_per_patch=15, maxactive_fraction=2.0,
+                 rng=np.random.default_rng(3))
+        tasks = D.checkout_batch(sc, 10, ntry=50)
+        assert len(tasks) == 3 and sc.sparse
+        assert not np.any(sc.sourcecat["is_valid"]) and sc.seed_weight().sum() == 0
+        assert sc.checkout_region()[1] is None
+        assert D.checkout_batch(sc, 5) == []
