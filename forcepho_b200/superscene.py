@@ -29,7 +29,9 @@ removed ``np.float``, so its own random draw fails on a fresh scene); draws
 use a seedable ``numpy.random.Generator``; ``convert_pa`` wraps angles into
 [-pi/2, pi/2] as its docstring says (the reference's loop compares with
 +pi/2 on both sides and, for the default even ``max_try``, returns its
-input).  The state file is written with this package's FITS writer.
+input); a random draw with every source checked out gives no region instead
+of normalising zero weights.  The state file is written with this package's
+FITS writer.
 """
 
 import json
