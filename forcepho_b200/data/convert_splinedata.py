@@ -21,7 +21,6 @@ Usage::
 """
 
 import os
-import struct
 import sys
 
 import numpy as np

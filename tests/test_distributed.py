@@ -6,7 +6,6 @@ import os
 import socket
 
 import numpy as np
-import pytest
 
 from forcepho_b200.distributed import balance
 

@@ -3,7 +3,6 @@ the device proposal builder against Galaxy.proposal (GPU)."""
 
 import numpy as np
 import pytest
-from scipy.interpolate import RectBivariateSpline
 
 from forcepho_b200.splines import default_splines
 
