@@ -154,3 +154,19 @@ def test_store_patch_subpatch_repacks_its_own_metadata(tmp_path):
     rest = D.exposure_subpatch(p, [0, 3])
     c = O.evaluate(sub, prop, precision="f64")[0] + O.evaluate(rest, prop, precision="f64")[0]
     assert np.allclose(c, c_all, rtol=1e-12, atol=0)
+
+
+def test_more_ranks_than_exposures():
+    """With 7 ranks for 6 exposures one rank holds nothing: it evaluates
+    nothing and contributes zeros, and the parts still add up."""
+    p, prop = _patch()
+    c_all, g_all, scale = _scale(p, prop)
+    parts = [D.SplitPatchProposer(p, r, 7, proposer=_OracleProposer(), send=False) for r in range(7)]
+    assert sum(1 for sp in parts if sp.patch is None) == 1
+    total = sum(sp.evaluate_local(prop) for sp in parts)
+    empty = [sp for sp in parts if sp.patch is None][0]
+    assert not np.any(empty.evaluate_local(prop))
+    c, g = parts[0].unpack(total)
+    assert np.max(np.abs(c - c_all)) <= 1e-12 * scale
+    for k in range(7):
+        assert np.linalg.norm(g[..., k] - g_all[..., k]) <= 1e-6 * np.linalg.norm(g_all[..., k])
