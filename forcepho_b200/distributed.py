@@ -190,7 +190,8 @@ class SplitPatchProposer:
     one ``all_reduce`` (sum) of n_bands x (1 + 7 n_sources) doubles gives every
     rank the whole patch's ``(chi2 f64[n_bands], chi2_derivs f32[n_bands,
     n_sources, 7])``, the shapes of ``GPUProposer.evaluate_proposal``.  The
-    sums are taken in FP64 and rounded to FP32 once.  With NCCL the reduced
+    ranks' chi2 (FP64) and FP32 gradients are summed in FP64, and the
+    gradient sums rounded to FP32 once more.  With NCCL the reduced
     buffer lives on the current CUDA device; with gloo on the host.  Every
     rank must call ``evaluate_proposal`` with the same proposal, in the same
     order (it is a collective).
