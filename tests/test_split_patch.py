@@ -40,8 +40,12 @@ def _scale(p, prop):
 def test_partition_sums_to_the_whole_patch(world):
     p, prop = _patch()
     c_all, g_all, scale = _scale(p, prop)
-    parts = D.balance(D.exposure_weights(p), world)
+    w = D.exposure_weights(p)
+    assert int(w.sum()) == p.n_pairs()
+    parts = D.balance(w, world)
     assert sorted(sum(parts, [])) == list(range(p.n_exp))
+    # largest first onto the least-loaded rank: no rank above the mean plus the largest exposure
+    assert max(sum(w[i] for i in part) for part in parts) <= w.sum() / world + w.max()
     c_sum = np.zeros_like(c_all)
     g_sum = np.zeros_like(g_all, dtype=np.float64)
     for ex in parts:
